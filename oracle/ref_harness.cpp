@@ -1,0 +1,132 @@
+/*
+ * Runs the reference's own device programs on the CPU — TEST INFRASTRUCTURE ONLY.
+ * oracle/Makefile compiles this file three times against sources in the reference tree
+ * (REF_STAGE 1: cuda_train/forward/gaussians_aabb.cu, 2: cuda_train/backward/gaussians_aabb.cu,
+ * 3: vec_math.h + utils/sh_utils.cu), with ref_shim/optix.h standing in for the OptiX device
+ * API.  The outputs (oracle/_ref/*.so) pin the C restatement in rg_oracle_impl.h.
+ */
+#include <cstring>
+#include <cstdlib>
+#include <cmath>
+
+#if REF_STAGE == 1 || REF_STAGE == 2
+#include REF_SOURCE
+thread_local RgEmulRay rg_emul;
+RgEmulScene rg_emul_scene;
+
+static void set_common(int n, const float* pos, const float* scl, const float* quat, const float* dens,
+                       const float* rgb, const float* scene_box, const float* cam, int W, int H,
+                       int max_prim_slice, int jitter, int rnd_sample, unsigned iteration, int* hit_buf) {
+    params.iteration = iteration;
+    params.jitter = (unsigned)jitter;
+    params.rnd_sample = (unsigned)rnd_sample;
+    params.max_prim_slice = (unsigned)max_prim_slice;
+    params.bbox_min = make_float3(scene_box[0], scene_box[1], scene_box[2]);
+    params.bbox_max = make_float3(scene_box[3], scene_box[4], scene_box[5]);
+    params.image_width = (unsigned)W;
+    params.image_height = (unsigned)H;
+    params.cam_eye = make_float3(cam[0], cam[1], cam[2]);
+    params.cam_u = make_float3(cam[3], cam[4], cam[5]);
+    params.cam_v = make_float3(cam[6], cam[7], cam[8]);
+    params.cam_w = make_float3(cam[9], cam[10], cam[11]);
+    params.cam_tan_half_fovx = cam[12];
+    params.cam_tan_half_fovy = cam[13];
+    params.densities = const_cast<float*>(dens);
+    params.color_features = const_cast<float*>(rgb);
+    params.positions = (float3*)pos;
+    params.scales = (float3*)scl;
+    params.quaternions = (float4*)quat;
+    params.hit_prim_idx = hit_buf;
+    (void)n;
+}
+
+static sphere::SphereHitGroupData g_sbt;
+
+static void run_rays(int n_rays, int W, int H) {
+#pragma omp parallel for schedule(dynamic, 8)
+    for (int r = 0; r < n_rays; ++r) {
+        rg_emul.launch_idx = make_uint3((unsigned)r, 0u, 0u);
+        rg_emul.launch_dim = make_uint3((unsigned)(W * H), 1u, 1u);
+        rg_emul.have_cands = false;
+        __raygen__rg();
+    }
+}
+#endif
+
+#if REF_STAGE == 1
+extern "C" int ref_forward(int n, const float* pos, const float* scl, const float* quat, const float* dens,
+                           const float* rgb, const float* aabb, const float* scene_box, const float* cam,
+                           int W, int H, int white_bg, int max_prim_slice, int jitter, int rnd_sample,
+                           unsigned iteration, float* out_colors, int* overflow) {
+    int* hit_buf = (int*)std::calloc((size_t)W * H * (size_t)max_prim_slice, sizeof(int));
+    if (!hit_buf) return -1;
+    set_common(n, pos, scl, quat, dens, rgb, scene_box, cam, W, H, max_prim_slice, jitter, rnd_sample,
+               iteration, hit_buf);
+    params.ray_colors = (float3*)out_colors;
+    params.handle = 0;
+    *overflow = 0;
+    params.max_gaussians_exceeded = overflow;
+    params.white_background = (unsigned)white_bg;
+    g_sbt.positions = (float3*)pos; g_sbt.scales = (float3*)scl; g_sbt.quaternions = (float4*)quat;
+    rg_emul_scene.aabb = aabb; rg_emul_scene.n = n; rg_emul_scene.sbt_data = &g_sbt;
+    run_rays(W * H, W, H);
+    std::free(hit_buf);
+    return 0;
+}
+#elif REF_STAGE == 2
+extern "C" int ref_backward(int n, const float* pos, const float* scl, const float* quat, const float* dens,
+                            const float* rgb, const float* aabb, const float* scene_box, const float* cam,
+                            int W, int H, int max_prim_slice, int jitter, int rnd_sample, unsigned iteration,
+                            const float* ray_colors, const float* dL, float* d_dens, float* d_rgb,
+                            float* d_pos, float* d_scl, float* d_quat) {
+    int* hit_buf = (int*)std::calloc((size_t)W * H * (size_t)max_prim_slice, sizeof(int));
+    if (!hit_buf) return -1;
+    set_common(n, pos, scl, quat, dens, rgb, scene_box, cam, W, H, max_prim_slice, jitter, rnd_sample,
+               iteration, hit_buf);
+    params.ray_colors = (float3*)ray_colors;
+    params.dloss_dray_colors = (float3*)dL;
+    params.densities_grad = d_dens;
+    params.color_features_grad = (float3*)d_rgb;
+    params.positions_grad = (float3*)d_pos;
+    params.scales_grad = (float3*)d_scl;
+    params.quaternions_grad = (float4*)d_quat;
+    params.handle = 0;
+    g_sbt.positions = (float3*)pos; g_sbt.scales = (float3*)scl; g_sbt.quaternions = (float4*)quat;
+    rg_emul_scene.aabb = aabb; rg_emul_scene.n = n; rg_emul_scene.sbt_data = &g_sbt;
+    run_rays(W * H, W, H);
+    std::free(hit_buf);
+    return 0;
+}
+#elif REF_STAGE == 3
+#include <vector_types.h>
+static thread_local uint3 threadIdx;
+static thread_local uint3 blockIdx;
+static thread_local dim3 blockDim;
+#include REF_VECMATH
+#include REF_SOURCE
+
+extern "C" void ref_forward_sh(const float* campos, const float* pos, const float* sh, const float* sg,
+                               const float* kappa, const float* axis, unsigned nsg, int deg, int n, float* rgb) {
+    blockDim = dim3(128, 1, 1);
+    for (int i = 0; i < n; ++i) {
+        blockIdx = make_uint3((unsigned)(i / 128), 0, 0);
+        threadIdx = make_uint3((unsigned)(i % 128), 0, 0);
+        forward_sh(const_cast<float*>(campos), (float3*)pos, const_cast<float*>(sh), const_cast<float*>(sg),
+                   const_cast<float*>(kappa), const_cast<float*>(axis), nsg, deg, n, rgb);
+    }
+}
+
+extern "C" void ref_backward_sh(const float* campos, const float* pos, const float* sh, const float* sg,
+                                const float* kappa, const float* axis, unsigned nsg, int deg, int n,
+                                const float* drgb, float* dsh, float* dpos, float* dsg, float* dkappa,
+                                float* daxis) {
+    blockDim = dim3(128, 1, 1);
+    for (int i = 0; i < n; ++i) {
+        blockIdx = make_uint3((unsigned)(i / 128), 0, 0);
+        threadIdx = make_uint3((unsigned)(i % 128), 0, 0);
+        backward_sh(const_cast<float*>(campos), (float3*)pos, const_cast<float*>(sh), const_cast<float*>(sg),
+                    const_cast<float*>(kappa), const_cast<float*>(axis), nsg, deg, n, (float3*)drgb, dsh,
+                    (float3*)dpos, dsg, dkappa, daxis);
+    }
+}
+#endif
