@@ -1,0 +1,427 @@
+"""Benchmark: forward+backward Mrays/s of the differentiable Gaussian ray caster on the 1M-Gaussian
+unbounded scene with 16 views of uneven resolution (the batched, BF16-storage form), next to the
+plain FP32 single-view drop-in form on the same views, the reference algorithm on the host cores
+and the HBM roofline of the dominant kernel.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--views V]
+
+A step is one training iteration of the hot path over the batch: pre-pass + LBVH build + colour
+pass + forward launch + MSE loss + backward launch + SH/SG backward and gradient assembly.  Inputs
+(parameters 460 MB FP32 / 314 MB BF16-stored) are larger than the 126 MB L2, so no flush is needed
+between timed steps.  Multi-GPU runs are independent replicas (one GPU renders the whole batch;
+the path needs no exchange), timed as the max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "fwd+bwd Mrays/s @1M Gaussians: plain FP32 vs batched+BF16 at PSNR Δ≤0.05 dB"
+WORKLOAD = "unbounded_1m"
+
+
+def _dist():
+    rank = int(os.environ.get("RANK", 0))
+    world = int(os.environ.get("WORLD_SIZE", 1))
+    local = int(os.environ.get("LOCAL_RANK", 0))
+    return rank, world, local
+
+
+def _clock_sampler(gpu_index):
+    q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+    try:
+        return subprocess.Popen(["nvidia-smi", "-i", str(gpu_index), f"--query-gpu={q}", "--format=csv,noheader,nounits",
+                                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+    except OSError:
+        return None
+
+
+def _clock_summary(proc):
+    if proc is None:
+        return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+    proc.terminate()
+    try:
+        out, _ = proc.communicate(timeout=5)
+    except subprocess.TimeoutExpired:
+        proc.kill()
+        out, _ = proc.communicate()
+    sm, mx, reasons = [], None, set()
+    names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+    for line in out.strip().splitlines():
+        f = [x.strip() for x in line.split(",")]
+        if len(f) < 9:
+            continue
+        try:
+            sm.append(float(f[1]))
+            mx = float(f[2])
+        except ValueError:
+            continue
+        for nm, v in zip(names, f[5:9]):
+            if v.lower() == "active":
+                reasons.add(nm)
+    return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
+            "samples": len(sm)}
+
+
+def _peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def bytes_per_gaussian(nsg, sh_coeffs, bf16):
+    """Storage bytes of one Gaussian's parameters (positions, scales, quaternion, density, SH, SG)."""
+    amp = 2 if bf16 else 4
+    return 12 + 12 + 16 + amp + 3 * sh_coeffs * amp + nsg * (3 * amp + 4 + 12)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--views", type=int, default=16)
+    ap.add_argument("--n", type=int, default=1_000_000)
+    ap.add_argument("--no-plain", action="store_true", help="skip the plain single-view comparison")
+    ap.add_argument("--no-cpu", action="store_true", help="skip the host-core baseline")
+    ap.add_argument("--cpu-rays", type=int, default=256, help="rays per view in the host-core sample")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    rank, world, local = _dist()
+    if args.impl == "reference":
+        return reference_arm(args, rank, world)
+    return our_arm(args, rank, world, local)
+
+
+def _setup(args, device):
+    import torch
+    from ray_gauss_b200 import synthetic as S
+    p, cams, white = S.workload(WORKLOAD, seed=0, device="cpu", n=args.n)
+    cams = cams[: args.views]
+    cams = [c.to(device) for c in cams]
+    P32 = {k: v.to(device) for k, v in p.items()}
+    return p, P32, cams, white
+
+
+def _bf16(P32):
+    import torch
+    P = dict(P32)
+    for k in ("densities", "color_features", "sph_gauss_features"):
+        P[k] = P32[k].to(torch.bfloat16)
+    return P
+
+
+def our_arm(args, rank, world, local):
+    import torch
+    from ray_gauss_b200.batched import BatchedRenderFunction, BatchedViews
+    from ray_gauss_b200.engine import Engine
+    from ray_gauss_b200.optix_raycasting.render_optix import RenderOptixFunction, RenderOptixSettings
+
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if world > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120))
+    p_host, P32, cams, white = _setup(args, dev)
+    n = P32["positions"].shape[0]
+    eng = Engine(local)
+    views = BatchedViews(cams, white_background=white, mode="fast", engine=eng)
+    R = views.n_rays
+    eng.reserve(n, len(cams), R)
+    Pb = _bf16(P32)
+    leaves = {k: v.clone().requires_grad_(True) for k, v in Pb.items()}
+    g = torch.Generator(device=dev)
+    g.manual_seed(1)
+    target = torch.rand((R, 3), device=dev, generator=g)
+
+    def step_batched(P):
+        out = BatchedRenderFunction.apply(P["positions"], P["scales"], P["quaternions"], P["densities"],
+                                          P["color_features"], P["sph_gauss_features"], P["bandwidth_sharpness"],
+                                          P["lobe_axis"], views)
+        loss = torch.nn.functional.mse_loss(out, target)
+        loss.backward()
+        return loss
+
+    def zero(P):
+        for v in P.values():
+            v.grad = None
+
+    def barrier():
+        if world > 1:
+            import torch.distributed as dist
+            dist.barrier()
+
+    # ---- headline: batched BF16-storage form (device-resident inputs) ----
+    for _ in range(args.warmup):
+        zero(leaves)
+        step_batched(leaves)
+    torch.cuda.synchronize()
+    eng.status(reset=True)
+    eng.timers = {}
+    launches0 = eng.kernel_launches()
+    clocks = _clock_sampler(local) if rank == 0 else None
+    barrier()
+    torch.cuda.synchronize()
+    t0 = torch.cuda.Event(enable_timing=True)
+    t1 = torch.cuda.Event(enable_timing=True)
+    t0.record()
+    for _ in range(args.steps):
+        zero(leaves)
+        step_batched(leaves)
+    t1.record()
+    torch.cuda.synchronize()
+    barrier()
+    clk = _clock_summary(clocks) if rank == 0 else None
+    ms = t0.elapsed_time(t1) / args.steps
+    launches = eng.kernel_launches() - launches0
+    timers, eng.timers = eng.timers, None
+    st = eng.status()
+    ms_max = ms
+    if world > 1:
+        import torch.distributed as dist
+        t = torch.tensor([ms], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms_max = float(t.item())
+    value = world * R / (ms_max * 1e-3) / 1e6
+
+    # dominant kernel: the backward launch (events on the launching stream)
+    bwd_ms = statistics.mean(a.elapsed_time(b) for a, b in timers["launch_backward"])
+    fwd_ms = statistics.mean(a.elapsed_time(b) for a, b in timers["launch_forward"])
+    prep_ms = statistics.mean(a.elapsed_time(b) for a, b in timers["prepare"])
+    shb_ms = statistics.mean(a.elapsed_time(b) for a, b in timers["backward_sh"])
+    nsg = P32["sph_gauss_features"].shape[2]
+    ncoef = P32["color_features"].shape[2]
+    V = len(cams)
+    # algorithmic bytes of one backward launch: leaf records (64 B) + scale/quaternion (32 B) + colour per
+    # view (16 B) read once per Gaussian, gradient accumulators written once (48 B + 16 B per view), ray
+    # colour and dL/dcolour read once per ray (24 B)
+    alg_bwd = n * (64 + 32 + 16 * V) + n * (48 + 16 * V) + 24 * R
+    peak, peak_kind = _peaks()
+    achieved = alg_bwd / (bwd_ms * 1e-3) / 1e9
+    roofline = {"bound": "hbm", "achieved": round(achieved, 2), "peak": peak, "unit": "GB/s",
+                "frac": round(achieved / peak, 5), "traffic": None, "peak_source": peak_kind,
+                "kernel": "k_render<backward> (rg_launch_backward)",
+                "algorithmic_bytes_per_launch": int(alg_bwd)}
+    # step-level algorithmic bytes (parameters read twice, gradients written once, 36 B per ray)
+    p_store = bytes_per_gaussian(nsg, ncoef, True)
+    g_bytes = bytes_per_gaussian(nsg, ncoef, False)
+    b_step = 2 * n * p_store + n * g_bytes + 36 * R
+
+    # ---- e2e through the public API: host parameters and targets in, loss out ----
+    e2e = None
+    if rank == 0 or True:
+        host = {k: v.detach().cpu().pin_memory() for k, v in Pb.items()}
+        host_target = target.cpu().pin_memory()
+        dev_buf = {k: torch.empty_like(v) for k, v in Pb.items()}
+        tgt_dev = torch.empty_like(target)
+        h2d = sum(v.numel() * v.element_size() for v in host.values()) + host_target.numel() * 4
+        loss_host = torch.empty((), dtype=torch.float32).pin_memory()
+
+        def step_e2e():
+            for k in host:
+                dev_buf[k].copy_(host[k], non_blocking=True)
+            tgt_dev.copy_(host_target, non_blocking=True)
+            P = {k: v.requires_grad_(True) for k, v in dev_buf.items()}
+            out = BatchedRenderFunction.apply(P["positions"], P["scales"], P["quaternions"], P["densities"],
+                                              P["color_features"], P["sph_gauss_features"],
+                                              P["bandwidth_sharpness"], P["lobe_axis"], views)
+            loss = torch.nn.functional.mse_loss(out, tgt_dev)
+            loss.backward()
+            loss_host.copy_(loss.detach(), non_blocking=True)
+            for v in P.values():
+                v.grad = None
+                v.requires_grad_(False)
+
+        for _ in range(2):
+            step_e2e()
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(max(2, args.steps // 2)):
+            step_e2e()
+        e1.record()
+        torch.cuda.synchronize()
+        e_ms = e0.elapsed_time(e1) / max(2, args.steps // 2)
+        e2e = {"value": round(world * R / (e_ms * 1e-3) / 1e6, 3), "unit": "Mrays/s", "h2d_bytes_per_step": int(h2d),
+               "d2h_bytes_per_step": 4, "ms_per_step": round(e_ms, 3)}
+
+    # ---- plain FP32 single-view drop-in form on the same views ----
+    plain = None
+    if not args.no_plain:
+        Pp = {k: v.clone().requires_grad_(True) for k, v in P32.items()}
+        tviews = [target[views.offsets[v]:views.offsets[v + 1]] for v in range(V)]
+
+        def step_plain():
+            for v, cam in enumerate(cams):
+                s = RenderOptixSettings(eng, False, None, None, None, None, None, cam, 1024, nsg, 0, 0, 0, (1, 1),
+                                        white, None, mode="parity")
+                img = RenderOptixFunction.apply(Pp["positions"], Pp["scales"], Pp["quaternions"], Pp["densities"],
+                                                Pp["color_features"], Pp["sph_gauss_features"],
+                                                Pp["bandwidth_sharpness"], Pp["lobe_axis"], s)
+                loss = torch.nn.functional.mse_loss(img, tviews[v])
+                loss.backward()
+
+        step_plain()
+        torch.cuda.synchronize()
+        p0 = torch.cuda.Event(enable_timing=True)
+        p1 = torch.cuda.Event(enable_timing=True)
+        psteps = max(1, args.steps // 2)
+        p0.record()
+        for _ in range(psteps):
+            zero(Pp)
+            step_plain()
+        p1.record()
+        torch.cuda.synchronize()
+        p_ms = p0.elapsed_time(p1) / psteps
+        plain = {"value": round(R / (p_ms * 1e-3) / 1e6, 3), "unit": "Mrays/s", "ms_per_step": round(p_ms, 3),
+                 "form": "RenderOptixFunction per view, FP32 storage, parity arithmetic"}
+
+    # ---- accuracy of the headline form: PSNR against the FP64 oracle on 64x64 crops (reported) ----
+    accuracy = None
+    cpu_baseline = None
+    if rank == 0 and not args.no_cpu:
+        accuracy, cpu_baseline = _host_side(args, p_host, cams, white, views, leaves, Pb, eng)
+
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank != 0:
+        return 0
+    line = {
+        "metric": METRIC, "value": round(value, 3), "unit": "Mrays/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": round(ms_max, 3), "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": f"{WORKLOAD}: {n} Gaussians (80% unit ball, 20% log-uniform radius 1-50), SH3 + "
+                               f"{nsg} SG, {V} views 400x300..1600x1200, batched one launch, BF16-stored "
+                               "density/SH/SG, fast arithmetic",
+                   "gaussians": n, "views": V, "rays_per_step": R, "storage": "bf16", "arith": "f32",
+                   "parallelism": f"replicas{world}", "l2": "inputs larger than L2 (no flush)"},
+        "e2e": e2e, "gpu_launches": int(launches // max(1, args.steps)) * args.steps,
+        "gpu_launches_per_step": int(launches // max(1, args.steps)),
+        "roofline": roofline,
+        "step_roofline": {"algorithmic_bytes": int(b_step), "achieved_gbs": round(b_step / (ms_max * 1e-3) / 1e9, 2),
+                          "frac": round(b_step / (ms_max * 1e-3) / 1e9 / peak, 5)},
+        "stage_ms": {"prepare(bbox+bvh+colour)": round(prep_ms, 3), "forward": round(fwd_ms, 3),
+                     "backward": round(bwd_ms, 3), "backward_sh": round(shb_ms, 3)},
+        "counters_per_step": {k: v // max(1, args.steps) for k, v in st.items()},
+        "plain_fp32_single_view": plain,
+        "batched_over_plain": round(value / world / plain["value"], 3) if plain else None,
+        "accuracy": accuracy,
+        "cpu_baseline": cpu_baseline,
+        "clocks": clk,
+    }
+    print(json.dumps(line))
+    return 0
+
+
+def _host_side(args, p_host, cams, white, views, leaves, Pb, eng):
+    """PSNR of the headline form against the FP64 oracle on seeded 64x64 crops, and the host-core baseline."""
+    import torch
+    from oracle import oracle as O
+    rng = np.random.default_rng(7)
+    n = p_host["positions"].shape[0]
+    # one rendered batch of the headline form (already computed in the timed loop; re-render once)
+    with torch.no_grad():
+        from ray_gauss_b200.batched import BatchedRenderFunction
+        out = BatchedRenderFunction.apply(*(Pb[k] for k in ("positions", "scales", "quaternions", "densities",
+                                                            "color_features", "sph_gauss_features",
+                                                            "bandwidth_sharpness", "lobe_axis")), views)
+    imgs = views.split(out.float().cpu())
+    Pn = {k: v.float().cpu().numpy() for k, v in Pb.items()}
+    acc = []
+    t_cpu, rays_cpu = 0.0, 0
+    threads = O.num_threads()
+    for v in range(min(2, len(cams))):
+        cam = cams[v]
+        W, H = cam.image_width, cam.image_height
+        cv = O.camera_vector(cam)
+        rgb = O.forward_sh(cv[:3], Pn["positions"], Pn["color_features"], Pn["sph_gauss_features"],
+                           Pn["bandwidth_sharpness"], Pn["lobe_axis"])
+        aabb, box = O.bbox(Pn["positions"], Pn["scales"], Pn["quaternions"], Pn["densities"], "f32")
+        x0, y0 = int(rng.integers(0, W - 64)), int(rng.integers(0, H - 64))
+        ids = np.array([(y0 + j) * W + (x0 + i) for j in range(64) for i in range(64)], np.int32)
+        ids = ids[:: max(1, len(ids) // args.cpu_rays)][: args.cpu_rays]
+        t = time.perf_counter()
+        img32, _, _ = O.render_forward(Pn["positions"], Pn["scales"], Pn["quaternions"], Pn["densities"], rgb, cv, W,
+                                       H, white, ray_ids=ids, aabb=aabb, scene_box=box, prec="f32")
+        dL = np.full(img32.shape, 1e-3, np.float32)
+        O.render_backward(Pn["positions"], Pn["scales"], Pn["quaternions"], Pn["densities"], rgb, cv, W, H, img32, dL,
+                          ray_ids=ids, aabb=aabb, scene_box=box, prec="f32")
+        t_cpu += time.perf_counter() - t
+        rays_cpu += len(ids)
+        img64, _, _ = O.render_forward(Pn["positions"], Pn["scales"], Pn["quaternions"], Pn["densities"], rgb, cv, W,
+                                       H, white, ray_ids=ids, prec="f64")
+        gpu = imgs[v].reshape(-1, 3).numpy()[ids]
+        mse = float(np.mean((gpu.astype(np.float64) - img64) ** 2))
+        acc.append({"view": v, "psnr_vs_fp64_oracle_db": (99.0 if mse == 0 else round(-10 * math.log10(mse), 2)),
+                    "max_abs": float(np.abs(gpu - img64).max()), "rays": int(len(ids))})
+    cpu = {"value": round(rays_cpu / t_cpu / 1e6, 6), "unit": "Mrays/s", "cores": threads, "kind": "port",
+           "sample": f"{rays_cpu} rays from seeded 64x64 crops of {min(2, len(cams))} views, FP32 forward+backward "
+                     "with the C restatement (brute-force candidate list per ray)"}
+    return acc, cpu
+
+
+def reference_arm(args, rank, world):
+    """The reference's CPU implementation of the path on the host cores (oracle/_ref when built here,
+    else the C restatement), bounded sample, same metric and unit."""
+    if rank != 0:
+        return 0
+    from oracle import oracle as O
+    from ray_gauss_b200 import synthetic as S
+    p, cams, white = S.workload(WORKLOAD, seed=0, device="cpu", n=args.n)
+    cams = cams[: args.views]
+    Pn = {k: v.numpy().astype(np.float32) for k, v in p.items()}
+    cam = cams[0]
+    W, H = cam.image_width, cam.image_height
+    cv = O.camera_vector(cam)
+    rgb = O.forward_sh(cv[:3], Pn["positions"], Pn["color_features"], Pn["sph_gauss_features"],
+                       Pn["bandwidth_sharpness"], Pn["lobe_axis"])
+    aabb, box = O.bbox(Pn["positions"], Pn["scales"], Pn["quaternions"], Pn["densities"], "f32")
+    rng = np.random.default_rng(3)
+    times = []
+    rays = max(16, args.cpu_rays // 4)
+    for s in range(args.warmup + args.steps):
+        ids = rng.integers(0, W * H, rays).astype(np.int32)
+        t = time.perf_counter()
+        img, _, _ = O.render_forward(Pn["positions"], Pn["scales"], Pn["quaternions"], Pn["densities"], rgb, cv, W, H,
+                                     white, ray_ids=ids, aabb=aabb, scene_box=box, prec="f32")
+        O.render_backward(Pn["positions"], Pn["scales"], Pn["quaternions"], Pn["densities"], rgb, cv, W, H, img,
+                          np.full(img.shape, 1e-3, np.float32), ray_ids=ids, aabb=aabb, scene_box=box, prec="f32")
+        if s >= args.warmup:
+            times.append(time.perf_counter() - t)
+    ms = statistics.mean(times) * 1e3
+    value = rays / (ms * 1e-3) / 1e6
+    line = {"impl": "reference", "metric": METRIC, "value": round(value, 6), "unit": "Mrays/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms, 3), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": f"{WORKLOAD} view 0, {rays} random rays per step"},
+            "cpu_baseline": {"value": round(value, 6), "unit": "Mrays/s", "cores": O.num_threads(), "kind": "port",
+                             "sample": f"{rays} random rays of view 0 per step, FP32 forward+backward"},
+            "e2e": {"value": round(value, 6), "unit": "Mrays/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,206 @@
+/*
+ * raygauss_b200 — C ABI of the B200 (sm_100a) engine for RayGauss's differentiable volumetric
+ * Gaussian ray caster.
+ *
+ * Plain C: pointers, sizes and POD structs only.  Every device pointer is borrowed (the caller
+ * owns it); the engine owns only its scratch (BVH, leaf records, per-view colours, gradient
+ * accumulators, work counters).  Every call is ordered on the CUDA stream passed as `stream`
+ * (a cudaStream_t, 0 = legacy default stream), performs no host synchronisation and no
+ * allocation once the engine has been sized for the scene (rg_reserve), and returns RG_OK or
+ * an RG_ERR_* code.  Device-side conditions (hit-list passes, stack overflow, watchdog,
+ * non-finite input) are counted in a device status block read by rg_get_status().
+ *
+ * Reference interfaces replaced (paths inside the reference project):
+ *   rg_ellipsoids_bbox  optix_raycasting/optix_utils.py:34-66 (quaternion_to_rotation,
+ *                       compute_ellipsoids_bbox) + render_optix.py:105-106 (scene box min/max)
+ *   rg_bvh_build        optix_raycasting/optix_utils.py:68-71 (create_acceleration_structure)
+ *   rg_bvh_refit        optix_raycasting/optix_utils.py:73-75 (update_acceleration_structure)
+ *   rg_forward_sh       utils/sh_utils.cu:25-119 (forward_sh) via render_optix.py:19-32
+ *                       (compute_cupy_rgb)
+ *   rg_launch_forward   optix_raycasting/optix_utils.py:128-209 (launch_pipeline_forward) and the
+ *                       programs of cuda_train/forward/gaussians_aabb.cu:324-641
+ *   rg_launch_backward  optix_raycasting/optix_utils.py:213-299 (launch_pipeline_backward) and the
+ *                       programs of cuda_train/backward/gaussians_aabb.cu:405-802
+ *   rg_backward_sh      utils/sh_utils.cu:121-315 (backward_sh) via render_optix.py:34-52
+ *                       (compute_cupy_sh_grad) and the gradient assembly of render_optix.py:170-190
+ *   rg_render_forward   RenderOptixFunction.forward, optix_raycasting/render_optix.py:92-132
+ *   rg_render_backward  RenderOptixFunction.backward, optix_raycasting/render_optix.py:136-190
+ */
+#ifndef RAYGAUSS_B200_H
+#define RAYGAUSS_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define RG_ABI_VERSION 1
+
+#if defined(__GNUC__)
+#define RG_API __attribute__((visibility("default")))
+#else
+#define RG_API
+#endif
+
+enum rg_result {
+    RG_OK = 0,
+    RG_ERR_INVALID_ARG = 1,   /* null pointer, bad size, unsupported degree, misaligned buffer */
+    RG_ERR_CUDA = 2,          /* a CUDA runtime call failed (see rg_last_cuda_error) */
+    RG_ERR_OOM = 3,           /* scratch allocation failed */
+    RG_ERR_STATE = 4,         /* call order violated (e.g. render before bbox/bvh) */
+    RG_ERR_CAPACITY = 5       /* request exceeds a fixed capacity of the entry point */
+};
+
+/* Storage type of densities, colour features and SG amplitudes. */
+enum rg_storage { RG_STORAGE_F32 = 0, RG_STORAGE_BF16 = 1 };
+
+/* Sample arithmetic of the render kernels.
+ * RG_MODE_PARITY: the reference's per-sample arithmetic (drop-in; image max-abs <= 1e-4).
+ * RG_MODE_FAST: incremental per-slab sample evaluation and moment-form adjoint (same sample
+ * grid, masks and early exit; accuracy reported as PSNR against the FP64 oracle). */
+enum rg_mode { RG_MODE_PARITY = 0, RG_MODE_FAST = 1 };
+
+/* Pinhole camera: the launch-parameter record of optix_utils.py:166-177.  u, v, w are the camera
+ * x (right), y (down) and z (forward) axes in world space, i.e. world_view_transform[:3,0..2];
+ * width/height are the ray grid (image size times supersampling). 64 bytes. */
+typedef struct rg_camera {
+    float eye[3];
+    float u[3];
+    float v[3];
+    float w[3];
+    float tan_half_fovx;
+    float tan_half_fovy;
+    int32_t width;
+    int32_t height;
+} rg_camera;
+
+/* Gaussian parameters in the layout of PointCloud.get_data (classes/point_cloud.py:729-739).
+ * All pointers are device pointers, contiguous, 4-byte aligned (16-byte for quaternions). */
+typedef struct rg_gaussians {
+    const float* positions;            /* (N,3) */
+    const float* scales;               /* (N,3), already exp(log_scale) */
+    const float* quaternions;          /* (N,4), (w,x,y,z), used as passed (not normalised) */
+    const void* densities;             /* (N,) raw, f32 or bf16 per `storage` */
+    const void* color_features;        /* (N,3,(deg+1)^2) channel-major, f32 or bf16 */
+    const void* sph_gauss_features;    /* (N,3,nsg), f32 or bf16; may be NULL when nsg == 0 */
+    const float* bandwidth_sharpness;  /* (N,nsg) after softplus; may be NULL when nsg == 0 */
+    const float* lobe_axis;            /* (N,nsg,3) unit axes; may be NULL when nsg == 0 */
+    int64_t n;
+    int32_t sh_degree;                 /* 0..3 */
+    int32_t num_sph_gauss;             /* 0..RG_MAX_SG */
+    int32_t storage;                   /* enum rg_storage */
+    int32_t reserved;
+} rg_gaussians;
+
+#define RG_MAX_SG 16
+
+/* Per-call settings: the RenderOptixSettings fields that reach the device
+ * (render_optix.py:67-87; configs/base.yml training.max_prim_slice/jitter/rnd_sample). */
+typedef struct rg_settings {
+    int32_t white_background;
+    int32_t jitter;
+    int32_t rnd_sample;
+    int32_t max_prim_slice;            /* reference per-slab hit cap (counted, never truncated) */
+    uint32_t iteration;                /* RNG seed component (tea<4>(iteration, ray)) */
+    int32_t mode;                      /* enum rg_mode */
+    int32_t sh_quirk;                  /* 1: reproduce the reference SH basis-9 y-derivative */
+    int32_t reserved;
+} rg_settings;
+
+/* Output gradients (device, f32, fully overwritten — no accumulation, no zero-fill needed).
+ * sph_gauss_features / bandwidth_sharpness / lobe_axis may be NULL when nsg == 0. */
+typedef struct rg_gradients {
+    float* positions;                  /* (N,3) geometric + view-direction terms */
+    float* scales;                     /* (N,3) */
+    float* quaternions;                /* (N,4) */
+    float* densities;                  /* (N,) */
+    float* color_features;             /* (N,3,(deg+1)^2) */
+    float* sph_gauss_features;         /* (N,3,nsg) */
+    float* bandwidth_sharpness;        /* (N,nsg) */
+    float* lobe_axis;                  /* (N,nsg,3) */
+} rg_gradients;
+
+/* Device counters accumulated since the last reset. */
+typedef struct rg_status {
+    uint64_t hit_pairs;                /* (ray, slab, Gaussian) pairs evaluated */
+    uint64_t slabs;                    /* (ray, slab) pairs marched */
+    uint64_t slab_cap_exceeded;        /* slabs with more hits than max_prim_slice (reference truncates) */
+    uint64_t list_passes;              /* extra traversal passes caused by a full warp hit list */
+    uint64_t chunk_splits;             /* chunk-length reductions caused by a full warp hit list */
+    uint64_t stack_overflows;          /* traversal stack overflows (result incomplete) */
+    uint64_t watchdog_trips;           /* work items abandoned by the iteration limit */
+    uint64_t nonfinite_inputs;         /* Gaussians with a non-finite parameter (skipped) */
+} rg_status;
+
+/* Kernel tuning knobs (rg_autotune picks them; 0 = keep the current value). */
+typedef struct rg_tuning {
+    int32_t chunk_slabs;               /* slabs per traversal chunk, 1..8 */
+    int32_t blocks_per_sm;             /* resident render CTAs per SM */
+    int32_t list_capacity;             /* warp hit-list capacity: 64, 128 or 256 */
+    int32_t reserved;
+} rg_tuning;
+
+typedef struct rg_engine rg_engine;
+
+/* Engine lifetime (no reference counterpart beyond create_context, optix_utils.py:77-81). */
+RG_API int rg_create(rg_engine** out, int device);
+RG_API int rg_destroy(rg_engine* e);
+/* Size the engine's scratch for n Gaussians, up to n_views views and n_rays rays per call.
+ * Calls made afterwards with sizes within these bounds allocate nothing. */
+RG_API int rg_reserve(rg_engine* e, int64_t n, int32_t n_views, int64_t n_rays);
+RG_API int rg_set_tuning(rg_engine* e, const rg_tuning* t);
+RG_API int rg_get_tuning(const rg_engine* e, rg_tuning* t);
+
+/* optix_utils.py:34-66 + render_optix.py:105-106.  Computes the per-Gaussian threshold-ellipsoid
+ * AABBs, the scene box and the leaf records used by the BVH and the render kernels.
+ * aabb_out (N,6) and scene_box_out (6) are optional device outputs (NULL to skip). */
+RG_API int rg_ellipsoids_bbox(rg_engine* e, const rg_gaussians* g, float* aabb_out, float* scene_box_out,
+                       void* stream);
+/* optix_utils.py:68-71: full LBVH build (Morton codes, radix sort, Karras hierarchy, refit). */
+RG_API int rg_bvh_build(rg_engine* e, void* stream);
+/* optix_utils.py:73-75: keep the leaf order and topology of the last build, refit the boxes to
+ * the current parameters (rg_ellipsoids_bbox must have run on the new parameters). */
+RG_API int rg_bvh_refit(rg_engine* e, void* stream);
+
+/* utils/sh_utils.cu:25-119 for n_cams views at once.  cams is a DEVICE array of rg_camera.
+ * rgb_out (n_cams,N,3) is an optional device output in Gaussian order. */
+RG_API int rg_forward_sh(rg_engine* e, const rg_gaussians* g, const rg_camera* cams, int32_t n_cams,
+                  float* rgb_out, void* stream);
+
+/* optix_utils.py:128-209 for n_cams views in one persistent launch.  ray_colors (R,3) with the
+ * views' rays packed in order, ray y*W+x within a view; final_T (R,) optional. */
+RG_API int rg_launch_forward(rg_engine* e, const rg_camera* cams, int32_t n_cams, const rg_settings* s,
+                      float* ray_colors, float* final_T, void* stream);
+/* optix_utils.py:213-299: re-traverse and scatter per-Gaussian gradients into the engine's
+ * accumulators (zeroed by this call).  ray_colors are the forward outputs. */
+RG_API int rg_launch_backward(rg_engine* e, const rg_camera* cams, int32_t n_cams, const rg_settings* s,
+                       const float* ray_colors, const float* dloss_dray_colors, void* stream);
+/* utils/sh_utils.cu:121-315 + render_optix.py:170-190: SH/SG backward for every view and the
+ * final gradient assembly into `out`. */
+RG_API int rg_backward_sh(rg_engine* e, const rg_gaussians* g, const rg_camera* cams, int32_t n_cams,
+                   const rg_settings* s, const rg_gradients* out, void* stream);
+
+/* RenderOptixFunction.forward (render_optix.py:92-132): bbox -> BVH (build, or refit when
+ * `refit` != 0 and a build of the same N exists) -> colour -> march.  rgb_out optional. */
+RG_API int rg_render_forward(rg_engine* e, const rg_gaussians* g, const rg_camera* cams, int32_t n_cams,
+                      const rg_settings* s, int32_t refit, float* ray_colors, float* final_T,
+                      float* rgb_out, void* stream);
+/* RenderOptixFunction.backward (render_optix.py:136-190) on the BVH and colours of the last
+ * rg_render_forward with the same parameters. */
+RG_API int rg_render_backward(rg_engine* e, const rg_gaussians* g, const rg_camera* cams, int32_t n_cams,
+                       const rg_settings* s, const float* ray_colors, const float* dloss_dray_colors,
+                       const rg_gradients* out, void* stream);
+
+/* Read (and optionally reset) the device counters; synchronises the engine's last stream. */
+RG_API int rg_get_status(rg_engine* e, rg_status* out, int32_t reset, void* stream);
+/* Number of kernels launched by this engine since creation (for launch accounting). */
+RG_API uint64_t rg_kernel_launches(const rg_engine* e);
+RG_API const char* rg_error_string(int code);
+RG_API const char* rg_last_cuda_error(const rg_engine* e);
+RG_API int rg_abi_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* RAYGAUSS_B200_H */

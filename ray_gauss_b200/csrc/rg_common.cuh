@@ -1,0 +1,113 @@
+// Shared device definitions of the B200 ray-caster engine.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <cuda_bf16.h>
+#include <stdint.h>
+
+#include "raygauss_b200.h"
+
+namespace rg {
+
+// Reference constants (optix_raycasting/cuda_train/forward/gaussians_aabb.h:2-5).
+constexpr int kBuf = 8;                 // samples per slab
+constexpr float kDt = 0.0025f;          // sample spacing
+constexpr float kSlab = kDt * kBuf;     // slab length (0.02)
+constexpr float kTeps = 0.003f;         // early-exit transmittance
+constexpr float kSigThr = 0.1f;         // per-sample density threshold
+
+constexpr int kWarp = 32;
+constexpr int kTileW = 8;               // a warp renders an 8x4 pixel tile
+constexpr int kTileH = 4;
+constexpr int kMaxChunk = 8;            // slabs per traversal chunk (mask bits per entry)
+constexpr int kStack = 96;              // warp traversal stack depth
+
+// Device status block (mirrors rg_status) + work counters.
+struct DevStatus {
+    unsigned long long hit_pairs;
+    unsigned long long slabs;
+    unsigned long long slab_cap_exceeded;
+    unsigned long long list_passes;
+    unsigned long long chunk_splits;
+    unsigned long long stack_overflows;
+    unsigned long long watchdog_trips;
+    unsigned long long nonfinite_inputs;
+};
+
+// Per-launch view table computed on the device from the camera array (no host sync).
+struct ViewTable {
+    int n_views;
+    int total_tiles;
+    long long total_rays;
+    int tile_prefix[65];
+    long long ray_prefix[65];
+};
+constexpr int kMaxViews = 64;
+
+// ---- small float3 helpers (own definitions) -------------------------------------------------
+__host__ __device__ __forceinline__ float3 f3(float x, float y, float z) { return make_float3(x, y, z); }
+__device__ __forceinline__ float3 operator+(float3 a, float3 b) { return f3(a.x + b.x, a.y + b.y, a.z + b.z); }
+__device__ __forceinline__ float3 operator-(float3 a, float3 b) { return f3(a.x - b.x, a.y - b.y, a.z - b.z); }
+__device__ __forceinline__ float3 operator*(float3 a, float s) { return f3(a.x * s, a.y * s, a.z * s); }
+__device__ __forceinline__ float dot3(float3 a, float3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+
+// Ordered-int encoding so that float min/max can use integer atomics.
+__device__ __forceinline__ int f2ord(float f) {
+    int i = __float_as_int(f);
+    return i >= 0 ? i : i ^ 0x7fffffff;
+}
+__host__ __device__ __forceinline__ float ord2f(int i) {
+#ifdef __CUDA_ARCH__
+    return __int_as_float(i >= 0 ? i : i ^ 0x7fffffff);
+#else
+    union { int i; float f; } u;
+    u.i = i >= 0 ? i : i ^ 0x7fffffff;
+    return u.f;
+#endif
+}
+
+__device__ __forceinline__ float load_param(const void* p, long long i, int storage) {
+    if (storage == RG_STORAGE_BF16) return __bfloat162float(reinterpret_cast<const __nv_bfloat16*>(p)[i]);
+    return reinterpret_cast<const float*>(p)[i];
+}
+
+// 2^x with the SFU (one MUFU.EX2); inputs here are <= 0 and the result may flush to zero.
+__device__ __forceinline__ float ex2_approx(float x) {
+    float y;
+    asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+
+// tea<4>(v0, v1) seeding and LCG draws of the reference RNG (forward/gaussians_aabb.h:63-94).
+__device__ __forceinline__ unsigned tea4(unsigned v0, unsigned v1) {
+    unsigned s0 = 0;
+#pragma unroll
+    for (int n = 0; n < 4; ++n) {
+        s0 += 0x9e3779b9u;
+        v0 += ((v1 << 4) + 0xa341316cu) ^ (v1 + s0) ^ ((v1 >> 5) + 0xc8013ea4u);
+        v1 += ((v0 << 4) + 0xad90777du) ^ (v0 + s0) ^ ((v0 >> 5) + 0x7e95761eu);
+    }
+    return v0;
+}
+__device__ __forceinline__ float lcg_rnd(unsigned& prev) {
+    prev = 1664525u * prev + 1013904223u;
+    return (float)(prev & 0x00FFFFFFu) / (float)0x01000000;
+}
+
+// Leaf record (leaf order), 64 bytes: {mu.xyz, density}, {M row 0, k}, {M row 1, 0}, {M row 2, 0}
+// where m = M (x - mu) = S^-1 R^T (x - mu) and k = 1/sqrt(log((density/0.1)^2)) scales M to the
+// threshold ellipsoid (forward/gaussians_aabb.cu:341-357).
+struct __align__(16) LeafRec {
+    float4 a, r0, r1, r2;
+};
+
+// BVH internal node, 64 bytes: child boxes, child ids (>= 0 internal, < 0 leaf ~id),
+// split position and last leaf of the node's range.
+struct __align__(16) Node {
+    float4 n0;  // lbox lo.xyz, lbox hi.x
+    float4 n1;  // lbox hi.yz, rbox lo.xy
+    float4 n2;  // rbox lo.z, rbox hi.xyz
+    int4 n3;    // left, right, split, range_hi
+};
+
+}  // namespace rg

@@ -1,0 +1,250 @@
+"""Parity of the sm_100a engine with the reference (golden fixtures) and with the CPU oracle.
+
+Tolerances: the drop-in (mode "parity", FP32) must match the reference with image max-abs <= 1e-4
+and gradient relative L2 <= 1e-3; the fast mode is held to max-abs <= 1e-3 / rel-L2 <= 1e-2 against
+the reference and reports PSNR against the FP64 oracle.
+"""
+import numpy as np
+import pytest
+import torch
+
+from conftest import SCENES, load_golden
+from helpers import camera_from_vector, psnr, rel_l2
+
+pytestmark = pytest.mark.gpu
+
+IMG_TOL = 1e-4
+GRAD_TOL = 1e-3
+
+
+def _params(c, dev, grad=True):
+    P = {k[3:]: torch.tensor(c[k], dtype=torch.float32, device=dev) for k in c if k.startswith("in_")}
+    for v in P.values():
+        v.requires_grad_(grad)
+    return P
+
+
+def _render(P, cam, *, mode="parity", white=True, max_prim_slice=1024, jitter=0, rnd_sample=0, iteration=0,
+            update=False, engine=None):
+    from ray_gauss_b200.optix_raycasting.render_optix import RenderOptixFunction, RenderOptixSettings
+    nsg = P["sph_gauss_features"].shape[2]
+    s = RenderOptixSettings(engine, update, None, None, None, None, None, cam, max_prim_slice, nsg, iteration, jitter,
+                            rnd_sample, (1, 1), white, None, mode=mode)
+    return RenderOptixFunction.apply(P["positions"], P["scales"], P["quaternions"], P["densities"],
+                                     P["color_features"], P["sph_gauss_features"], P["bandwidth_sharpness"],
+                                     P["lobe_axis"], s)
+
+
+def _run_golden(c, dev, mode):
+    P = _params(c, dev)
+    cam = camera_from_vector(c["cam"], int(c["width"]), int(c["height"]), dev)
+    img = _render(P, cam, mode=mode, white=bool(c["white"]), max_prim_slice=int(c["max_prim_slice"]),
+                  jitter=int(c["jitter"]), rnd_sample=int(c["rnd_sample"]), iteration=int(c["iteration"]))
+    img.backward(torch.tensor(c["dL"], device=dev))
+    torch.cuda.synchronize()
+    return img.detach().cpu().numpy(), {k: (v.grad.cpu().numpy() if v.grad is not None else None) for k, v in P.items()}
+
+
+GRAD_KEYS = [("positions", "ref_d_pos"), ("scales", "ref_d_scl"), ("quaternions", "ref_d_quat"),
+             ("densities", "ref_d_dens"), ("color_features", "ref_d_sh")]
+SG_KEYS = [("sph_gauss_features", "ref_d_sg"), ("bandwidth_sharpness", "ref_d_kappa"), ("lobe_axis", "ref_d_axis")]
+
+
+@pytest.mark.parametrize("name", SCENES)
+def test_parity_mode_matches_reference(cuda, name):
+    c = load_golden(name)
+    img, g = _run_golden(c, cuda, "parity")
+    assert np.abs(img - c["ref_image"]).max() <= IMG_TOL
+    keys = GRAD_KEYS + (SG_KEYS if c["in_sph_gauss_features"].shape[2] else [])
+    for k, ref in keys:
+        assert rel_l2(g[k], c[ref]) <= GRAD_TOL, (k, rel_l2(g[k], c[ref]))
+
+
+@pytest.mark.parametrize("name", [s for s in SCENES if s in ("small_object_sh3", "shells_sg8", "inside_camera")])
+def test_fast_mode_close_to_reference(cuda, oracle, name):
+    c = load_golden(name)
+    img, g = _run_golden(c, cuda, "fast")
+    assert np.abs(img - c["ref_image"]).max() <= 1e-3
+    keys = GRAD_KEYS + (SG_KEYS if c["in_sph_gauss_features"].shape[2] else [])
+    for k, ref in keys:
+        assert rel_l2(g[k], c[ref]) <= 1e-2, (k, rel_l2(g[k], c[ref]))
+    P = {k[3:]: c[k] for k in c if k.startswith("in_")}
+    img64, _, _ = oracle.render_forward(P["positions"], P["scales"], P["quaternions"], P["densities"], c["ref_rgb"],
+                                        c["cam"], int(c["width"]), int(c["height"]), bool(c["white"]), prec="f64")
+    assert psnr(img, img64) >= 60.0
+
+
+def _config1(dev, n=10_000, W=200, H=200, seed=0):
+    from ray_gauss_b200 import synthetic as S
+    p, cams, white = S.workload("small_object", seed=seed, n=n)
+    cam = S.sphere_camera(3.0, W, H, 40.0, seed, device=dev)
+    P = {k: v.to(dev).requires_grad_(True) for k, v in p.items()}
+    return P, cam, white
+
+
+@pytest.mark.parametrize("mode", ["parity", "fast"])
+def test_small_object_full_size_against_oracle(cuda, oracle, mode):
+    """The 10k-Gaussian, 200x200 workload against the FP32 restatement (and FP64 for PSNR)."""
+    P, cam, white = _config1(cuda)
+    img = _render(P, cam, mode=mode, white=white)
+    rng = np.random.default_rng(5)
+    dL = torch.tensor(rng.normal(0, 1e-4, (img.shape[0], 3)), dtype=torch.float32, device=cuda)
+    img.backward(dL)
+    torch.cuda.synchronize()
+    Pn = {k: v.detach().cpu().numpy() for k, v in P.items()}
+    cv = oracle.camera_vector(cam)
+    rgb = oracle.forward_sh(cv[:3], Pn["positions"], Pn["color_features"], None, None, None)
+    ref, _, _ = oracle.render_forward(Pn["positions"], Pn["scales"], Pn["quaternions"], Pn["densities"], rgb, cv, 200,
+                                      200, white)
+    out = img.detach().cpu().numpy()
+    tol = IMG_TOL if mode == "parity" else 1e-3
+    assert np.abs(out - ref).max() <= tol
+    g = oracle.render_backward(Pn["positions"], Pn["scales"], Pn["quaternions"], Pn["densities"], rgb, cv, 200, 200,
+                               ref, dL.cpu().numpy())
+    gtol = GRAD_TOL if mode == "parity" else 1e-2
+    assert rel_l2(P["densities"].grad.cpu().numpy(), g["d_dens"]) <= gtol
+    assert rel_l2(P["scales"].grad.cpu().numpy(), g["d_scl"]) <= gtol
+    assert rel_l2(P["quaternions"].grad.cpu().numpy(), g["d_quat"]) <= gtol
+    dsh, dpos, _, _, _ = oracle.backward_sh(cv[:3], Pn["positions"], Pn["color_features"], None, None, None,
+                                            g["d_rgb"].astype(np.float32), ref_quirks=True)
+    assert rel_l2(P["color_features"].grad.cpu().numpy(), dsh) <= gtol
+    assert rel_l2(P["positions"].grad.cpu().numpy(), g["d_pos"] + dpos) <= gtol
+    ref64, _, _ = oracle.render_forward(Pn["positions"], Pn["scales"], Pn["quaternions"], Pn["densities"], rgb, cv,
+                                        200, 200, white, prec="f64")
+    assert psnr(out, ref64) >= 60.0
+
+
+def test_small_list_capacity_multi_pass_is_exact(cuda, oracle):
+    """A tiny warp hit list forces chunk splitting and multi-pass slabs; no hit may be lost."""
+    from ray_gauss_b200.engine import Engine
+    eng = Engine(cuda.index or 0)
+    eng.set_tuning(chunk_slabs=8, list_capacity=64)
+    c = load_golden("small_object_sh3")
+    P = _params(c, cuda)
+    cam = camera_from_vector(c["cam"], int(c["width"]), int(c["height"]), cuda)
+    eng.status(reset=True)
+    img = _render(P, cam, engine=eng)
+    img.backward(torch.tensor(c["dL"], device=cuda))
+    st = eng.status()
+    assert st["list_passes"] + st["chunk_splits"] > 0
+    assert st["stack_overflows"] == 0 and st["watchdog_trips"] == 0
+    assert np.abs(img.detach().cpu().numpy() - c["ref_image"]).max() <= IMG_TOL
+    for k, ref in GRAD_KEYS:
+        assert rel_l2(P[k].grad.cpu().numpy(), c[ref]) <= GRAD_TOL
+
+
+@pytest.mark.parametrize("chunk", [1, 3, 8])
+def test_chunk_length_does_not_change_the_image(cuda, chunk):
+    from ray_gauss_b200.engine import Engine
+    eng = Engine(cuda.index or 0)
+    eng.set_tuning(chunk_slabs=chunk, list_capacity=256)
+    c = load_golden("shells_sg8")
+    P = _params(c, cuda, grad=False)
+    cam = camera_from_vector(c["cam"], int(c["width"]), int(c["height"]), cuda)
+    img = _render(P, cam, engine=eng, white=bool(c["white"]))
+    assert np.abs(img.cpu().numpy() - c["ref_image"]).max() <= IMG_TOL
+
+
+def test_batched_views_equal_single_views(cuda):
+    """Three uneven views in one launch give the single-view images, and gradients sum."""
+    from ray_gauss_b200 import synthetic as S
+    from ray_gauss_b200.batched import BatchedRenderFunction, BatchedViews
+    p, _, _ = S.workload("small_object", n=3000, seed=3)
+    p["scales"] = p["scales"] * 2.0
+    cams = [S.sphere_camera(3.0, w, h, 40.0, seed=k, device=cuda) for k, (w, h) in enumerate([(40, 30), (17, 23), (64, 8)])]
+    P = {k: v.to(cuda).requires_grad_(True) for k, v in p.items()}
+    views = BatchedViews(cams, white_background=True, mode="parity")
+    out = BatchedRenderFunction.apply(P["positions"], P["scales"], P["quaternions"], P["densities"],
+                                      P["color_features"], P["sph_gauss_features"], P["bandwidth_sharpness"],
+                                      P["lobe_axis"], views)
+    dL = torch.randn_like(out) * 1e-3
+    out.backward(dL)
+    gb = {k: v.grad.clone() for k, v in P.items() if v.grad is not None}
+    singles = []
+    acc = {k: torch.zeros_like(v) for k, v in gb.items()}
+    for v, cam in enumerate(cams):
+        for t in P.values():
+            t.grad = None
+        img = _render(P, cam)
+        img.backward(dL[views.offsets[v]:views.offsets[v + 1]])
+        singles.append(img.detach())
+        for k in acc:
+            acc[k] += P[k].grad
+    assert torch.equal(torch.cat(singles), out.detach())
+    for k in acc:
+        assert rel_l2(gb[k].cpu().numpy(), acc[k].cpu().numpy()) <= 1e-5, k
+
+
+def test_refit_matches_rebuild(cuda):
+    from ray_gauss_b200.engine import Engine
+    eng = Engine(cuda.index or 0)
+    c = load_golden("small_object_sh3")
+    P = _params(c, cuda, grad=False)
+    cam = camera_from_vector(c["cam"], int(c["width"]), int(c["height"]), cuda)
+    _render(P, cam, engine=eng)
+    P2 = dict(P)
+    P2["positions"] = P["positions"] + 0.01 * torch.randn_like(P["positions"])
+    a = _render(P2, cam, engine=eng, update=True)
+    b = _render(P2, cam, engine=eng, update=False)
+    assert (a - b).abs().max().item() <= 1e-6
+
+
+def test_bf16_storage(cuda, oracle):
+    """SH/SG amplitudes and densities stored in BF16: the engine computes in FP32 on the rounded values."""
+    c = load_golden("shells_sg8")
+    P = _params(c, cuda, grad=False)
+    for k in ("densities", "color_features", "sph_gauss_features"):
+        P[k] = P[k].to(torch.bfloat16)
+    cam = camera_from_vector(c["cam"], int(c["width"]), int(c["height"]), cuda)
+    img = _render(P, cam, white=bool(c["white"])).cpu().numpy()
+    Pr = {k: v.float().cpu().numpy() for k, v in P.items()}
+    rgb = oracle.forward_sh(c["cam"][:3], Pr["positions"], Pr["color_features"], Pr["sph_gauss_features"],
+                            Pr["bandwidth_sharpness"], Pr["lobe_axis"])
+    ref, _, _ = oracle.render_forward(Pr["positions"], Pr["scales"], Pr["quaternions"], Pr["densities"], rgb, c["cam"],
+                                      int(c["width"]), int(c["height"]), bool(c["white"]))
+    assert np.abs(img - ref).max() <= IMG_TOL
+
+
+def test_edge_cases(cuda):
+    from ray_gauss_b200 import synthetic as S
+    dev = cuda
+    # one Gaussian (the BVH root is a leaf)
+    P = {k: torch.tensor(v, dtype=torch.float32, device=dev) for k, v in dict(
+        positions=[[0.0, 0.0, 0.0]], scales=[[0.2, 0.2, 0.2]], quaternions=[[1.0, 0.0, 0.0, 0.0]], densities=[3.0],
+        color_features=np.zeros((1, 3, 16)), sph_gauss_features=np.zeros((1, 3, 0)),
+        bandwidth_sharpness=np.zeros((1, 0)), lobe_axis=np.zeros((1, 0, 3))).items()}
+    cam = S.look_at_camera([0, 0, 3.0], [0, 0, 0], 16, 16, fovx=0.5, fovy=0.5, device=dev)
+    img = _render(P, cam)
+    assert torch.isfinite(img).all() and img.min().item() < 0.99
+    # all densities below the threshold: pure background
+    P["densities"] = torch.tensor([0.05], device=dev)
+    img = _render(P, cam, white=True)
+    assert torch.all(img == 1.0)
+    img = _render(P, cam, white=False)
+    assert torch.all(img == 0.0)
+    # camera looking away from the scene: background
+    P["densities"] = torch.tensor([3.0], device=dev)
+    cam2 = S.look_at_camera([0, 0, 3.0], [0, 0, 6.0], 8, 8, fovx=0.5, fovy=0.5, device=dev)
+    assert torch.all(_render(P, cam2) == 1.0)
+
+
+def test_nonfinite_input_is_counted_and_skipped(cuda):
+    from ray_gauss_b200.engine import Engine
+    eng = Engine(cuda.index or 0)
+    c = load_golden("small_object_sh3")
+    P = _params(c, cuda, grad=False)
+    P["positions"][3, 1] = float("nan")
+    cam = camera_from_vector(c["cam"], int(c["width"]), int(c["height"]), cuda)
+    eng.status(reset=True)
+    img = _render(P, cam, engine=eng)
+    assert torch.isfinite(img).all()
+    assert eng.status()["nonfinite_inputs"] == 1
+
+
+def test_render_is_deterministic_in_forward(cuda):
+    c = load_golden("inside_camera")
+    P = _params(c, cuda, grad=False)
+    cam = camera_from_vector(c["cam"], int(c["width"]), int(c["height"]), cuda)
+    a = _render(P, cam)
+    b = _render(P, cam)
+    assert torch.equal(a, b)
