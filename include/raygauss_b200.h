@@ -135,9 +135,9 @@ typedef struct rg_status {
 
 /* Kernel tuning knobs (rg_autotune picks them; 0 = keep the current value). */
 typedef struct rg_tuning {
-    int32_t chunk_slabs;               /* slabs per traversal chunk, 1..8 */
+    int32_t chunk_slabs;               /* longest traversal chunk in slabs, 1..255 */
     int32_t blocks_per_sm;             /* resident render CTAs per SM */
-    int32_t list_capacity;             /* warp hit-list capacity: 64, 128 or 256 */
+    int32_t list_capacity;             /* warp hit-list capacity: 64 or 128 */
     int32_t reserved;
 } rg_tuning;
 
@@ -192,6 +192,10 @@ RG_API int rg_render_backward(rg_engine* e, const rg_gaussians* g, const rg_came
                        const rg_settings* s, const float* ray_colors, const float* dloss_dray_colors,
                        const rg_gradients* out, void* stream);
 
+/* Leaf order of the last BVH build: leaf_gid_out[l] = index of the Gaussian in leaf l (N int32,
+ * device).  Hits of a slab are accumulated in increasing leaf order; the reference's order is
+ * its (unspecified) traversal order.  No reference counterpart (introspection of the BVH). */
+RG_API int rg_leaf_order(rg_engine* e, int32_t* leaf_gid_out, void* stream);
 /* Read (and optionally reset) the device counters; synchronises the engine's last stream. */
 RG_API int rg_get_status(rg_engine* e, rg_status* out, int32_t reset, void* stream);
 /* Number of kernels launched by this engine since creation (for launch accounting). */

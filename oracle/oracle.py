@@ -133,14 +133,17 @@ def backward_sh(campos, pos, sh, sg, kappa, axis, drgb, prec="f32", ref_quirks=T
 
 
 def render_forward(pos, scl, quat, dens, rgb, cam_vec, width, height, white_bg=True, max_prim_slice=1024,
-                   jitter=0, rnd_sample=0, iteration=0, ray_ids=None, aabb=None, scene_box=None, prec="f32"):
-    """Image (n_rays, 3) and final transmittance (n_rays,) of the reference forward pass."""
+                   jitter=0, rnd_sample=0, iteration=0, ray_ids=None, aabb=None, scene_box=None, prec="f32",
+                   order=None):
+    """Image (n_rays, 3) and final transmittance (n_rays,) of the reference forward pass.  ``order``
+    (optional permutation of the Gaussians) fixes the order in which a slab's hits are summed."""
     dt = _dt(prec)
     pos, scl, quat, dens, rgb = (_c(a, dt) for a in (pos, scl, quat, dens, rgb))
     if aabb is None or scene_box is None:
         aabb, scene_box = bbox(pos, scl, quat, dens, prec)
     aabb, scene_box, cam = _c(aabb, dt), _c(scene_box, dt), _c(cam_vec, dt)
     ids = None if ray_ids is None else _c(ray_ids, np.int32)
+    order = None if order is None else _c(order, np.int32)
     nr = width * height if ids is None else ids.shape[0]
     out = np.zeros((nr, 3), dt)
     out_t = np.zeros(nr, dt)
@@ -149,12 +152,13 @@ def render_forward(pos, scl, quat, dens, rgb, cam_vec, width, height, white_bg=T
         ctypes.c_int(pos.shape[0]), _p(pos), _p(scl), _p(quat), _p(dens), _p(rgb), _p(aabb), _p(scene_box),
         _p(cam), ctypes.c_int(width), ctypes.c_int(height), ctypes.c_int(int(bool(white_bg))),
         ctypes.c_int(max_prim_slice), ctypes.c_int(jitter), ctypes.c_int(rnd_sample),
-        ctypes.c_uint(iteration), _p(ids), ctypes.c_int(nr), _p(out), _p(out_t), _p(stats))
+        ctypes.c_uint(iteration), _p(ids), ctypes.c_int(nr), _p(order), _p(out), _p(out_t), _p(stats))
     return out, out_t, stats
 
 
 def render_backward(pos, scl, quat, dens, rgb, cam_vec, width, height, ray_colors, dL, max_prim_slice=1024,
-                    jitter=0, rnd_sample=0, iteration=0, ray_ids=None, aabb=None, scene_box=None, prec="f32"):
+                    jitter=0, rnd_sample=0, iteration=0, ray_ids=None, aabb=None, scene_box=None, prec="f32",
+                    order=None):
     """Hand adjoint of the reference: dict of d_rgb, d_dens, d_pos, d_scl, d_quat (float64)."""
     dt = _dt(prec)
     pos, scl, quat, dens, rgb = (_c(a, dt) for a in (pos, scl, quat, dens, rgb))
@@ -163,6 +167,7 @@ def render_backward(pos, scl, quat, dens, rgb, cam_vec, width, height, ray_color
     aabb, scene_box, cam = _c(aabb, dt), _c(scene_box, dt), _c(cam_vec, dt)
     ray_colors, dL = _c(ray_colors, dt), _c(dL, dt)
     ids = None if ray_ids is None else _c(ray_ids, np.int32)
+    order = None if order is None else _c(order, np.int32)
     nr = width * height if ids is None else ids.shape[0]
     n = pos.shape[0]
     g = {k: np.zeros(s, np.float64) for k, s in
@@ -171,7 +176,8 @@ def render_backward(pos, scl, quat, dens, rgb, cam_vec, width, height, ray_color
     getattr(_lib(), "orc_render_backward_" + prec)(
         ctypes.c_int(n), _p(pos), _p(scl), _p(quat), _p(dens), _p(rgb), _p(aabb), _p(scene_box), _p(cam),
         ctypes.c_int(width), ctypes.c_int(height), ctypes.c_int(max_prim_slice), ctypes.c_int(jitter),
-        ctypes.c_int(rnd_sample), ctypes.c_uint(iteration), _p(ids), ctypes.c_int(nr), _p(ray_colors), _p(dL),
+        ctypes.c_int(rnd_sample), ctypes.c_uint(iteration), _p(ids), ctypes.c_int(nr), _p(order), _p(ray_colors),
+        _p(dL),
         _p(g["d_rgb"]), _p(g["d_dens"]), _p(g["d_pos"]), _p(g["d_scl"]), _p(g["d_quat"]), _p(stats))
     g["stats"] = stats
     return g

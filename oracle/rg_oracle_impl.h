@@ -24,7 +24,9 @@
  * 0.003, SIGMA_THRESHOLD 0.1).  RNG: forward/gaussians_aabb.h:63-94.
  *
  * The traversal (OptiX BVH in the reference) is replaced by a brute-force candidate list per
- * ray: every Gaussian whose exact ellipsoid interval overlaps the ray's scene-box interval.
+ * ray: every Gaussian whose exact ellipsoid interval overlaps the ray's scene-box interval, in
+ * Gaussian index order or in a given order (e.g. a BVH leaf order, so that FP32 sums of a slab's
+ * hits associate the same way as in an engine that visits hits in that order).
  * The per-slab hit decision then uses the reference's exact interval test verbatim, so the set
  * of hits per slab is the reference's set (ordered by Gaussian index; the reference's order is
  * unspecified).  Gradients are accumulated in double in both instantiations.
@@ -52,8 +54,9 @@ static inline V3 ORC_FN(divs)(V3 a, REAL s) { REAL inv = (REAL)1 / s; return ORC
 #define DOT ORC_FN(dot)
 #define DIVS ORC_FN(divs)
 
-static inline REAL ORC_FN(r_exp)(REAL x) { return (sizeof(REAL) == 4) ? (REAL)expf((float)x) : (REAL)exp((double)x); }
-static inline REAL ORC_FN(r_log)(REAL x) { return (sizeof(REAL) == 4) ? (REAL)logf((float)x) : (REAL)log((double)x); }
+/* correctly rounded exponential: double exp rounded to REAL (for REAL=float this is expf rounded to nearest) */
+static inline REAL ORC_FN(r_exp)(REAL x) { return (REAL)exp((double)x); }
+static inline REAL ORC_FN(r_log)(REAL x) { return (REAL)log((double)x); }
 static inline REAL ORC_FN(r_sqrt)(REAL x) { return (sizeof(REAL) == 4) ? (REAL)sqrtf((float)x) : (REAL)sqrt((double)x); }
 #define REXP ORC_FN(r_exp)
 #define RLOG ORC_FN(r_log)
@@ -369,10 +372,11 @@ static inline int ORC_FN(slab_hit)(REAL lo, REAL hi, REAL r1, REAL r2) {
 /* All Gaussians whose exact interval overlaps [tenter, texit]; an AABB prefilter with a generous
  * margin only skips work (the exact test decides). */
 static int ORC_FN(gather_cands)(const SCENE* S, const REAL* aabb, V3 o, V3 d, REAL tenter, REAL texit,
-                                CAND* out) {
+                                const int* order, CAND* out) {
     int m = 0;
     V3 invd = MK((REAL)1 / d.x, (REAL)1 / d.y, (REAL)1 / d.z);
-    for (int g = 0; g < S->n; ++g) {
+    for (int li = 0; li < S->n; ++li) {
+        int g = order ? order[li] : li;
         const REAL* bb = aabb + 6 * g;
         double tn = tenter, tf = texit;
         double oo[3] = {o.x, o.y, o.z}, id[3] = {invd.x, invd.y, invd.z};
@@ -465,8 +469,8 @@ static int ORC_FN(slab_hits)(const CAND* cands, int nc, REAL lo, REAL hi, int ca
 int ORC_FN(orc_render_forward)(int n, const REAL* pos, const REAL* scl, const REAL* quat, const REAL* dens,
                                const REAL* rgb, const REAL* aabb, const REAL* scene_box, const REAL* cam,
                                int W, int H, int white_bg, int max_prim_slice, int jitter, int rnd_sample,
-                               unsigned iteration, const int* ray_ids, int n_rays, REAL* out, REAL* out_T,
-                               long long* stats) {
+                               unsigned iteration, const int* ray_ids, int n_rays, const int* order, REAL* out,
+                               REAL* out_T, long long* stats) {
     SCENE S = {pos, scl, quat, dens, rgb, n};
     long long st0 = 0, st1 = 0, st2 = 0;
     int cap = max_prim_slice > 0 ? max_prim_slice : 1024;
@@ -486,7 +490,7 @@ int ORC_FN(orc_render_forward)(int n, const REAL* pos, const REAL* scl, const RE
             REAL T = 1;
             V3 col = MK(0, 0, 0);
             if (tenter < texit) {
-                int nc = ORC_FN(gather_cands)(&S, aabb, o, d, tenter, texit, cands);
+                int nc = ORC_FN(gather_cands)(&S, aabb, o, d, tenter, texit, order, cands);
                 const REAL slab = ORC_DT * (REAL)ORC_BUF;
                 REAL tb = tenter;
                 while (tb < texit && T > ORC_TEPS) {
@@ -528,7 +532,7 @@ int ORC_FN(orc_render_forward)(int n, const REAL* pos, const REAL* scl, const RE
 int ORC_FN(orc_render_backward)(int n, const REAL* pos, const REAL* scl, const REAL* quat, const REAL* dens,
                                 const REAL* rgb, const REAL* aabb, const REAL* scene_box, const REAL* cam,
                                 int W, int H, int max_prim_slice, int jitter, int rnd_sample,
-                                unsigned iteration, const int* ray_ids, int n_rays,
+                                unsigned iteration, const int* ray_ids, int n_rays, const int* order,
                                 const REAL* ray_colors, const REAL* dL,
                                 double* drgb, double* ddens, double* dpos, double* dscl, double* dquat,
                                 long long* stats) {
@@ -548,7 +552,7 @@ int ORC_FN(orc_render_backward)(int n, const REAL* pos, const REAL* scl, const R
             REAL tenter, texit;
             ORC_FN(scene_clip)(scene_box, o, d, &tenter, &texit);
             if (!(tenter < texit)) continue;
-            int nc = ORC_FN(gather_cands)(&S, aabb, o, d, tenter, texit, cands);
+            int nc = ORC_FN(gather_cands)(&S, aabb, o, d, tenter, texit, order, cands);
             const REAL slab = ORC_DT * (REAL)ORC_BUF;
             REAL tb = tenter;
             REAL Tb = 1;

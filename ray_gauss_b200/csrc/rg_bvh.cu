@@ -22,7 +22,7 @@ __global__ void k_reset_box(int* scene_ord) {
 __global__ void __launch_bounds__(256) k_prepass(long long n, const float* __restrict__ pos,
                                                  const float* __restrict__ scl, const float4* __restrict__ quat,
                                                  const void* __restrict__ dens, int storage,
-                                                 LeafRec* __restrict__ rec, float* __restrict__ aabb,
+                                                 GaussRec* __restrict__ rec, float* __restrict__ aabb,
                                                  int* __restrict__ scene_ord, DevStatus* st) {
     long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     float lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
@@ -35,33 +35,54 @@ __global__ void __launch_bounds__(256) k_prepass(long long n, const float* __res
                       isfinite(sz) && isfinite(q.x) && isfinite(q.y) && isfinite(q.z) && isfinite(q.w) &&
                       isfinite(d);
         float w = q.x, x = q.y, y = q.z, z = q.w;
-        // rotation matrix R (rows) of the (w,x,y,z) polynomial (optix_utils.py:34-46)
-        float R00 = 1.f - 2.f * (y * y + z * z), R01 = 2.f * (x * y - w * z), R02 = 2.f * (x * z + w * y);
-        float R10 = 2.f * (x * y + w * z), R11 = 1.f - 2.f * (x * x + z * z), R12 = 2.f * (y * z - w * x);
-        float R20 = 2.f * (x * z - w * y), R21 = 2.f * (y * z + w * x), R22 = 1.f - 2.f * (x * x + y * y);
-        float ratio = d / 0.1f;
-        float lg = logf(ratio * ratio);
-        float delta = sqrtf(fmaxf(lg, 0.f));
-        float e0 = sqrtf((delta * sx * R00) * (delta * sx * R00) + (delta * sy * R01) * (delta * sy * R01) +
-                         (delta * sz * R02) * (delta * sz * R02));
-        float e1 = sqrtf((delta * sx * R10) * (delta * sx * R10) + (delta * sy * R11) * (delta * sy * R11) +
-                         (delta * sz * R12) * (delta * sz * R12));
-        float e2 = sqrtf((delta * sx * R20) * (delta * sx * R20) + (delta * sy * R21) * (delta * sy * R21) +
-                         (delta * sz * R22) * (delta * sz * R22));
-        float ix = 1.f / sx, iy = 1.f / sy, iz = 1.f / sz;
+        // Rotation matrix R of the (w,x,y,z) polynomial (optix_utils.py:34-46), the threshold scale
+        // and the AABB, in IEEE operation order (no contraction) so that the scene box, the slab grid
+        // anchored on it and the sample positions reproduce the FP32 reference arithmetic.
+#define MUL __fmul_rn
+#define ADD __fadd_rn
+#define SUB __fsub_rn
+        float R00 = SUB(1.f, MUL(2.f, ADD(MUL(y, y), MUL(z, z)))), R01 = MUL(2.f, SUB(MUL(x, y), MUL(w, z)));
+        float R02 = MUL(2.f, ADD(MUL(x, z), MUL(w, y))), R10 = MUL(2.f, ADD(MUL(x, y), MUL(w, z)));
+        float R11 = SUB(1.f, MUL(2.f, ADD(MUL(x, x), MUL(z, z)))), R12 = MUL(2.f, SUB(MUL(y, z), MUL(w, x)));
+        float R20 = MUL(2.f, SUB(MUL(x, z), MUL(w, y))), R21 = MUL(2.f, ADD(MUL(y, z), MUL(w, x)));
+        float R22 = SUB(1.f, MUL(2.f, ADD(MUL(x, x), MUL(y, y))));
+        float ratio = __fdiv_rn(d, 0.1f);
+        float lg = (float)log((double)MUL(ratio, ratio));   // correctly rounded log
+        float delta = __fsqrt_rn(fmaxf(lg, 0.f));
+        float ds0 = MUL(delta, sx), ds1 = MUL(delta, sy), ds2 = MUL(delta, sz);
+        float e00 = MUL(ds0, R00), e01 = MUL(ds1, R01), e02 = MUL(ds2, R02);
+        float e10 = MUL(ds0, R10), e11 = MUL(ds1, R11), e12 = MUL(ds2, R12);
+        float e20 = MUL(ds0, R20), e21 = MUL(ds1, R21), e22 = MUL(ds2, R22);
+        float e0 = __fsqrt_rn(ADD(ADD(MUL(e00, e00), MUL(e01, e01)), MUL(e02, e02)));
+        float e1 = __fsqrt_rn(ADD(ADD(MUL(e10, e10), MUL(e11, e11)), MUL(e12, e12)));
+        float e2 = __fsqrt_rn(ADD(ADD(MUL(e20, e20), MUL(e21, e21)), MUL(e22, e22)));
+        float ix = __fdiv_rn(1.f, sx), iy = __fdiv_rn(1.f, sy), iz = __fdiv_rn(1.f, sz);
         LeafRec r;
         // m_j = (column j of R) . (x - mu) / s_j
         r.a = make_float4(px, py, pz, d);
-        r.r0 = make_float4(R00 * ix, R10 * ix, R20 * ix, 1.f / sqrtf(lg));
-        r.r1 = make_float4(R01 * iy, R11 * iy, R21 * iy, 0.f);
-        r.r2 = make_float4(R02 * iz, R12 * iz, R22 * iz, 0.f);
+        r.r0 = make_float4(MUL(R00, ix), MUL(R10, ix), MUL(R20, ix), 1.f / sqrtf(lg));
+        r.r1 = make_float4(MUL(R01, iy), MUL(R11, iy), MUL(R21, iy), 0.f);
+        r.r2 = make_float4(MUL(R02, iz), MUL(R12, iz), MUL(R22, iz), 0.f);
+        float b[6] = {SUB(px, e0), SUB(py, e1), SUB(pz, e2), ADD(px, e0), ADD(py, e1), ADD(pz, e2)};
+        // reference intersection-program conic: s' = s sqrt(log(ratio^2)) (NaN below the threshold)
+        float dl_is = __fsqrt_rn(lg);
+        float jx = __fdiv_rn(1.f, MUL(sx, dl_is)), jy = __fdiv_rn(1.f, MUL(sy, dl_is)),
+              jz = __fdiv_rn(1.f, MUL(sz, dl_is));
+        LeafIS is;
+        is.u = make_float4(MUL(R00, jx), MUL(R10, jx), MUL(R20, jx), 0.f);
+        is.v = make_float4(MUL(R01, jy), MUL(R11, jy), MUL(R21, jy), 0.f);
+        is.w = make_float4(MUL(R02, jz), MUL(R12, jz), MUL(R22, jz), 0.f);
+#undef MUL
+#undef ADD
+#undef SUB
         if (!finite) {
             atomicAdd(&st->nonfinite_inputs, 1ull);
             r.a = make_float4(0.f, 0.f, 0.f, 0.f);
             r.r0.w = __int_as_float(0x7fc00000);  // NaN threshold factor: never hit
+            is.u.x = __int_as_float(0x7fc00000);
         }
-        rec[g] = r;
-        float b[6] = {px - e0, py - e1, pz - e2, px + e0, py + e1, pz + e2};
+        rec[g].s = r;
+        rec[g].is = is;
         if (aabb) {
             for (int a = 0; a < 6; ++a) aabb[6 * g + a] = finite ? b[a] : (a < 3 ? INFINITY : -INFINITY);
         }
@@ -136,15 +157,16 @@ __global__ void k_morton(long long n, const float* __restrict__ aabb, const int*
 
 // Leaf-ordered records and slightly inflated leaf boxes (the exact test decides; the boxes only
 // need to be conservative), plus the Gaussian -> leaf rank.
-__global__ void k_leaves(long long n, const int* __restrict__ leaf_gid, const LeafRec* __restrict__ rec,
+__global__ void k_leaves(long long n, const int* __restrict__ leaf_gid, const GaussRec* __restrict__ rec,
                          const float* __restrict__ aabb, const float* __restrict__ scl,
-                         const float4* __restrict__ quat, LeafRec* __restrict__ leaf_rec,
+                         const float4* __restrict__ quat, LeafRec* __restrict__ leaf_rec, LeafIS* __restrict__ leaf_is,
                          float4* __restrict__ leaf_ext, float4* __restrict__ leaf_lo, float4* __restrict__ leaf_hi,
                          int* __restrict__ rank) {
     long long l = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (l >= n) return;
     int g = leaf_gid[l];
-    leaf_rec[l] = rec[g];
+    leaf_rec[l] = rec[g].s;
+    leaf_is[l] = rec[g].is;
     rank[g] = (int)l;
     leaf_ext[2 * l] = make_float4(scl[3 * (long long)g], scl[3 * (long long)g + 1], scl[3 * (long long)g + 2], 0.f);
     leaf_ext[2 * l + 1] = quat[g];
@@ -237,7 +259,7 @@ __global__ void k_refit(int n, const float4* __restrict__ leaf_lo, const float4*
 
 // ---- host launchers --------------------------------------------------------------------------
 
-cudaError_t launch_prepass(const rg_gaussians* g, LeafRec* rec, float* aabb, int* scene_ord, DevStatus* st,
+cudaError_t launch_prepass(const rg_gaussians* g, GaussRec* rec, float* aabb, int* scene_ord, DevStatus* st,
                            cudaStream_t s) {
     k_reset_box<<<1, 32, 0, s>>>(scene_ord);
     long long n = g->n;
@@ -263,7 +285,7 @@ size_t sort_temp_bytes(long long n) {
 
 cudaError_t launch_refit_only(long long n, BvhBuffers& b, cudaStream_t s);
 
-cudaError_t launch_build(long long n, const float* aabb, const int* scene_ord, const LeafRec* rec,
+cudaError_t launch_build(long long n, const float* aabb, const int* scene_ord, const GaussRec* rec,
                          const rg_gaussians* g, BvhBuffers& b, cudaStream_t s) {
     int blocks = (int)((n + 255) / 256);
     k_morton<<<blocks, 256, 0, s>>>(n, aabb, scene_ord, b.keys_in, b.vals_in);
@@ -272,7 +294,7 @@ cudaError_t launch_build(long long n, const float* aabb, const int* scene_ord, c
                                                       b.leaf_gid, (int)n, 0, 63, s);
     if (err != cudaSuccess) return err;
     k_leaves<<<blocks, 256, 0, s>>>(n, b.leaf_gid, rec, aabb, g->scales, reinterpret_cast<const float4*>(g->quaternions),
-                                    b.leaf_rec, b.leaf_ext, b.leaf_lo, b.leaf_hi, b.rank);
+                                    b.leaf_rec, b.leaf_is, b.leaf_ext, b.leaf_lo, b.leaf_hi, b.rank);
     if (n > 1) {
         int ib = (int)((n - 1 + 255) / 256);
         k_karras<<<ib, 256, 0, s>>>((int)n, b.keys_out, b.nodes, b.leaf_parent, b.node_parent);
@@ -288,11 +310,11 @@ cudaError_t launch_refit_only(long long n, BvhBuffers& b, cudaStream_t s) {
     return cudaGetLastError();
 }
 
-cudaError_t launch_refit(long long n, const float* aabb, const LeafRec* rec, const rg_gaussians* g, BvhBuffers& b,
+cudaError_t launch_refit(long long n, const float* aabb, const GaussRec* rec, const rg_gaussians* g, BvhBuffers& b,
                          cudaStream_t s) {
     int blocks = (int)((n + 255) / 256);
     k_leaves<<<blocks, 256, 0, s>>>(n, b.leaf_gid, rec, aabb, g->scales, reinterpret_cast<const float4*>(g->quaternions),
-                                    b.leaf_rec, b.leaf_ext, b.leaf_lo, b.leaf_hi, b.rank);
+                                    b.leaf_rec, b.leaf_is, b.leaf_ext, b.leaf_lo, b.leaf_hi, b.rank);
     return launch_refit_only(n, b, s);
 }
 

@@ -14,7 +14,7 @@ struct rg_engine {
     long long cap_n = 0;
     int cap_views = 0;
     long long cap_rays = 0;
-    rg::LeafRec* rec = nullptr;      // Gaussian order
+    rg::GaussRec* rec = nullptr;     // Gaussian order
     float* aabb = nullptr;           // (N,6)
     int* scene_ord = nullptr;        // 6 ordered ints
     rg::BvhBuffers bvh;
@@ -28,7 +28,7 @@ struct rg_engine {
     long long n_built = -1;          // N of the last rg_bvh_build
     int colors_views = 0;            // views in the colour table
     rg_gaussians g_bbox{};           // parameters of the last rg_ellipsoids_bbox (borrowed pointers)
-    rg_tuning tuning{8, 0, 128, 0};
+    rg_tuning tuning{128, 0, 128, 0};
     unsigned long long launches = 0;
     char last_err[256] = {0};
 };
@@ -68,6 +68,7 @@ int ensure_n(rg_engine* e, long long n) {
     if ((rc = grow(e, e->bvh.leaf_gid, N))) return rc;
     if ((rc = grow(e, e->bvh.rank, N))) return rc;
     if ((rc = grow(e, e->bvh.leaf_rec, N))) return rc;
+    if ((rc = grow(e, e->bvh.leaf_is, N))) return rc;
     if ((rc = grow(e, e->bvh.leaf_ext, N * 2))) return rc;
     if ((rc = grow(e, e->bvh.leaf_lo, N))) return rc;
     if ((rc = grow(e, e->bvh.leaf_hi, N))) return rc;
@@ -141,6 +142,7 @@ int fill_args(rg_engine* e, const rg_camera* cams, const rg_settings* s, rg::Ren
     a.cams = cams;
     a.views = e->vt;
     a.rec = e->bvh.leaf_rec;
+    a.is_rec = e->bvh.leaf_is;
     a.ext = e->bvh.leaf_ext;
     a.rgb = e->rgb_leaf;
     a.nodes = e->bvh.nodes;
@@ -203,7 +205,7 @@ int rg_destroy(rg_engine* e) {
     if (!e) return RG_OK;
     set_device(e);
     void* ptrs[] = {e->rec, e->aabb, e->scene_ord, e->bvh.keys_in, e->bvh.keys_out, e->bvh.vals_in, e->bvh.leaf_gid,
-                    e->bvh.rank, e->bvh.leaf_rec, e->bvh.leaf_ext, e->bvh.leaf_lo, e->bvh.leaf_hi, e->bvh.nodes,
+                    e->bvh.rank, e->bvh.leaf_rec, e->bvh.leaf_is, e->bvh.leaf_ext, e->bvh.leaf_lo, e->bvh.leaf_hi, e->bvh.nodes,
                     e->bvh.leaf_parent, e->bvh.node_parent, e->bvh.refit_cnt, e->bvh.root_box, e->bvh.sort_temp,
                     e->rgb_leaf, e->gacc_geo, e->gacc_rgb, e->vt, e->work_counter, e->st};
     for (void* p : ptrs)
@@ -225,7 +227,7 @@ int rg_reserve(rg_engine* e, int64_t n, int32_t n_views, int64_t n_rays) {
 int rg_set_tuning(rg_engine* e, const rg_tuning* t) {
     if (!e || !t) return RG_ERR_INVALID_ARG;
     if (t->chunk_slabs < 0 || t->chunk_slabs > rg::kMaxChunk) return RG_ERR_INVALID_ARG;
-    if (t->list_capacity != 0 && t->list_capacity != 64 && t->list_capacity != 128 && t->list_capacity != 256)
+    if (t->list_capacity != 0 && t->list_capacity != 64 && t->list_capacity != 128)
         return RG_ERR_INVALID_ARG;
     if (t->blocks_per_sm < 0) return RG_ERR_INVALID_ARG;
     if (t->chunk_slabs) e->tuning.chunk_slabs = t->chunk_slabs;
@@ -377,6 +379,17 @@ int rg_render_backward(rg_engine* e, const rg_gaussians* g, const rg_camera* cam
     int rc = rg_launch_backward(e, cams, n_cams, s, ray_colors, dloss_dray_colors, stream);
     if (rc) return rc;
     return rg_backward_sh(e, g, cams, n_cams, s, out, stream);
+}
+
+int rg_leaf_order(rg_engine* e, int32_t* leaf_gid_out, void* stream) {
+    if (!e || !leaf_gid_out) return RG_ERR_INVALID_ARG;
+    if (e->n_built <= 0) return RG_ERR_STATE;
+    int rc = set_device(e);
+    if (rc) return rc;
+    RG_CUDA(cudaMemcpyAsync(leaf_gid_out, e->bvh.leaf_gid, sizeof(int32_t) * (size_t)e->n_built,
+                            cudaMemcpyDeviceToDevice, S(stream)),
+            "copy leaf order");
+    return RG_OK;
 }
 
 int rg_get_status(rg_engine* e, rg_status* out, int32_t reset, void* stream) {

@@ -122,13 +122,14 @@ __global__ void __launch_bounds__(128) k_color_bwd(long long n, const float* __r
     if (g >= n) return;
     const int nsh = (deg + 1) * (deg + 1);
     int leaf = rank[g];
+    // accumulator layout (12 floats): ddens, dpos.xyz, dscale.xyz, dquat.xyzw, pad
     float4 a0 = gacc_geo[3 * (long long)leaf], a1 = gacc_geo[3 * (long long)leaf + 1],
            a2 = gacc_geo[3 * (long long)leaf + 2];
     float dpos[3] = {a0.y, a0.z, a0.w};
     out.densities[g] = a0.x;
     out.scales[3 * g] = a1.x; out.scales[3 * g + 1] = a1.y; out.scales[3 * g + 2] = a1.z;
-    out.quaternions[4 * g] = a2.x; out.quaternions[4 * g + 1] = a2.y;
-    out.quaternions[4 * g + 2] = a2.z; out.quaternions[4 * g + 3] = a2.w;
+    out.quaternions[4 * g] = a1.w; out.quaternions[4 * g + 1] = a2.x;
+    out.quaternions[4 * g + 2] = a2.y; out.quaternions[4 * g + 3] = a2.z;
 
     float coef[3][16];
 #pragma unroll

@@ -19,7 +19,7 @@ constexpr float kSigThr = 0.1f;         // per-sample density threshold
 constexpr int kWarp = 32;
 constexpr int kTileW = 8;               // a warp renders an 8x4 pixel tile
 constexpr int kTileH = 4;
-constexpr int kMaxChunk = 8;            // slabs per traversal chunk (mask bits per entry)
+constexpr int kMaxChunk = 255;          // slabs per traversal chunk (slab ranges are bytes)
 constexpr int kStack = 96;              // warp traversal stack depth
 
 // Device status block (mirrors rg_status) + work counters.
@@ -99,6 +99,19 @@ __device__ __forceinline__ float lcg_rnd(unsigned& prev) {
 // threshold ellipsoid (forward/gaussians_aabb.cu:341-357).
 struct __align__(16) LeafRec {
     float4 a, r0, r1, r2;
+};
+
+// Threshold-ellipsoid conic of a leaf in the reference's arithmetic, 48 bytes: the rotation columns
+// scaled by 1/(s_j sqrt(log((density/0.1)^2))) (forward/gaussians_aabb.cu:341-357), used by the
+// exact ray/ellipsoid interval test of the parity arithmetic.
+struct __align__(16) LeafIS {
+    float4 u, v, w;
+};
+
+// Per-Gaussian pre-pass output in Gaussian order (gathered into leaf order by the BVH build).
+struct __align__(16) GaussRec {
+    LeafRec s;
+    LeafIS is;
 };
 
 // BVH internal node, 64 bytes: child boxes, child ids (>= 0 internal, < 0 leaf ~id),

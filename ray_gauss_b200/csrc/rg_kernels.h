@@ -12,6 +12,7 @@ struct BvhBuffers {
     int* leaf_gid = nullptr;      // leaf -> Gaussian
     int* rank = nullptr;          // Gaussian -> leaf
     LeafRec* leaf_rec = nullptr;  // leaf-ordered records
+    LeafIS* leaf_is = nullptr;    // leaf-ordered reference conics (parity intersection test)
     float4* leaf_ext = nullptr;   // leaf-ordered {scale.xyz, 0}, {quaternion}
     float4* leaf_lo = nullptr;
     float4* leaf_hi = nullptr;
@@ -28,6 +29,7 @@ struct RenderArgs {
     const rg_camera* cams;
     const ViewTable* views;
     const LeafRec* rec;
+    const LeafIS* is_rec;
     const float4* ext;
     const float4* rgb;            // (n_views, n_leaves) leaf order
     const Node* nodes;
@@ -42,19 +44,19 @@ struct RenderArgs {
     // backward inputs / outputs
     const float* ray_colors_in;
     const float* dL;
-    float4* gacc_geo;             // (n_leaves, 3): {ddens, dpos.xyz}, {dscale.xyz, 0}, {dquat}
+    float4* gacc_geo;             // (n_leaves, 3): ddens, dpos.xyz, dscale.xyz, dquat.xyzw, pad
     float4* gacc_rgb;             // (n_views, n_leaves): {drgb.xyz, 0}
     int* work_counter;
     DevStatus* st;
 };
 
-cudaError_t launch_prepass(const rg_gaussians* g, LeafRec* rec, float* aabb, int* scene_ord, DevStatus* st,
+cudaError_t launch_prepass(const rg_gaussians* g, GaussRec* rec, float* aabb, int* scene_ord, DevStatus* st,
                            cudaStream_t s);
 cudaError_t launch_scene_out(const int* scene_ord, float* out, cudaStream_t s);
 size_t sort_temp_bytes(long long n);
-cudaError_t launch_build(long long n, const float* aabb, const int* scene_ord, const LeafRec* rec,
+cudaError_t launch_build(long long n, const float* aabb, const int* scene_ord, const GaussRec* rec,
                          const rg_gaussians* g, BvhBuffers& b, cudaStream_t s);
-cudaError_t launch_refit(long long n, const float* aabb, const LeafRec* rec, const rg_gaussians* g,
+cudaError_t launch_refit(long long n, const float* aabb, const GaussRec* rec, const rg_gaussians* g,
                          BvhBuffers& b, cudaStream_t s);
 
 cudaError_t launch_setup_views(const rg_camera* cams, int n_cams, ViewTable* vt, int* work_counter,
@@ -65,7 +67,7 @@ cudaError_t launch_color_backward(const rg_gaussians* g, const rg_camera* cams, 
                                   const float4* gacc_geo, const float4* gacc_rgb, int sh_quirk,
                                   const rg_gradients* out, cudaStream_t s);
 
-// mode: RG_MODE_PARITY / RG_MODE_FAST; cap: 64/128/256
+// mode: RG_MODE_PARITY / RG_MODE_FAST; cap: 64/128
 cudaError_t launch_render(bool backward, int mode, int cap, int grid, const RenderArgs& a, cudaStream_t s);
 int render_block_threads();
 int render_occupancy(bool backward, int mode, int cap);

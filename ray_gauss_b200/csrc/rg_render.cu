@@ -11,17 +11,28 @@
 //   adjoint                   optix_raycasting/cuda_train/backward/gaussians_aabb.cu:505-775
 //
 // Design.  A warp owns an 8x4 pixel tile (tiles of all views are pulled from one atomic work
-// counter).  Each lane marches its own ray; the warp advances in chunks of up to 8 slabs per
-// lane.  For a chunk the warp traverses the LBVH once for the union of its lanes' segments with a
-// warp-uniform stack, runs the exact ellipsoid test per lane at the leaves and appends every leaf
-// that any lane hits to a shared hit list together with one 32-bit lane mask per slab.  The list
-// is then consumed slab by slab: every lane evaluates only the entries whose mask bit it owns,
-// reading the leaf record with a warp-uniform (broadcast) load.  A full list halves the chunk;
-// a full list for a single slab is consumed in several passes (a leaf-index cursor skips the
-// leaves already taken; DFS order visits leaves in increasing index), so no hit is ever dropped.
-// The adjoint recomputes each slab's sample buffers, folds the per-sample compositing adjoint
-// into three scalars per sample, evaluates each Gaussian's gradient per lane, reduces it across
-// the warp with shuffles and issues vector atomics (float4) into leaf-ordered accumulators.
+// counter).  Each lane marches its own ray with the reference's slab sequence (tb += 0.02 in
+// FP32); the warp advances in chunks of K slabs per lane (K adapts between 1 and 64: it grows
+// while hits are sparse and halves when the hit list overflows).  For a chunk the warp traverses
+// the LBVH once for the union of its lanes' segments with a warp-uniform stack, runs the exact
+// ellipsoid test per lane at the leaves and appends every leaf that any lane hits to a shared hit
+// list with, per lane, the range of the chunk's slabs its interval covers (exact for K <= 8; one
+// slab of margin on each side for longer chunks, where the extra slabs' samples fall outside the
+// threshold ellipsoid and are masked out).  The list is consumed slab by slab: each lane evaluates
+// only entries whose range holds the slab, reading the leaf record with a warp-uniform (broadcast)
+// load.  A full list for a single slab is consumed in several passes (a leaf-index cursor skips
+// the leaves already taken; DFS order visits leaves in increasing index), so no hit is dropped.
+// The adjoint recomputes each slab's sample buffers, folds the compositing adjoint into three
+// scalars per sample, evaluates each Gaussian's gradient per lane, reduces it across the warp with
+// a transposed shuffle reduction (16 shuffles for 14 values) and issues one atomic per value.
+//
+// Sample arithmetic.  RG_MODE_PARITY evaluates samples, ray generation and compositing in the
+// reference's operation order with IEEE round-to-nearest operations (no FMA contraction); when a
+// sample's density*weight lies within a few ulps of the 0.1 threshold the weight is re-evaluated
+// with a correctly rounded exponential so the threshold decision matches the FP32 reference
+// arithmetic.  RG_MODE_FAST evaluates the 8 samples of a slab from the quadratic form of the
+// Mahalanobis distance along the ray with the SFU exponential and accumulates the adjoint in
+// moment form.
 #include "rg_common.cuh"
 #include "rg_kernels.h"
 
@@ -31,11 +42,18 @@ constexpr int kWarpsPerBlock = 4;
 constexpr unsigned kFull = 0xffffffffu;
 constexpr int kMaxRounds = 1 << 20;        // chunk rounds per tile before the watchdog trips
 constexpr float kNegHalfLog2e = -0.72134752044448170f;
+constexpr float kInvSlab = 50.0f;          // 1 / 0.02
+constexpr int kExactChunk = 8;             // chunks up to this length use exact slab ranges
+
+constexpr int kMaskChunk = 128;            // longest chunk (slab entry masks are kept per slab)
 
 template <int CAP>
 struct WarpSmem {
     int ids[CAP];
-    unsigned mask[kMaxChunk][CAP];
+    unsigned urng[CAP];                    // union of the lanes' slab ranges: lo | hi << 16
+    unsigned short lrng[CAP][32];          // per lane: lo | hi << 8 (lo > hi: not hit)
+    unsigned smask[kMaskChunk][CAP / 32];  // entries whose union range holds slab k
+    unsigned long long occ[4];             // slabs holding any entry (union occupancy)
     int stack[kStack];
 };
 
@@ -49,6 +67,14 @@ struct RayState {
     unsigned seed;
     bool alive;
 };
+
+// ---- IEEE-ordered helpers (no contraction) for the parity arithmetic ----------------------------
+__device__ __forceinline__ float dot_rn(float3 a, float3 b) {
+    return __fadd_rn(__fadd_rn(__fmul_rn(a.x, b.x), __fmul_rn(a.y, b.y)), __fmul_rn(a.z, b.z));
+}
+__device__ __forceinline__ float3 rows_rn(float3 r0, float3 r1, float3 r2, float3 v) {
+    return f3(dot_rn(r0, v), dot_rn(r1, v), dot_rn(r2, v));
+}
 
 __device__ __forceinline__ bool box_hit(const float* bx, const RayState& r, float lo, float hi) {
     float tx0 = (bx[0] - r.o.x) * r.invd.x, tx1 = (bx[3] - r.o.x) * r.invd.x;
@@ -69,14 +95,133 @@ __device__ __forceinline__ LeafRec load_rec(const LeafRec* p, int i) {
     return r;
 }
 
+// Ray/ellipsoid interval in the reference intersection program's arithmetic
+// (forward/gaussians_aabb.cu:359-381): IEEE operations in source order on the precomputed
+// threshold-scaled conic.  Returns false when disc <= 1e-7 (no report).
+__device__ __forceinline__ bool roots_exact(const LeafIS& s, float3 mu, const RayState& r, float& root1,
+                                            float& root2) {
+    float3 U = f3(s.u.x, s.u.y, s.u.z), V = f3(s.v.x, s.v.y, s.v.z), W = f3(s.w.x, s.w.y, s.w.z);
+    float3 O = f3(__fsub_rn(r.o.x, mu.x), __fsub_rn(r.o.y, mu.y), __fsub_rn(r.o.z, mu.z));
+    float3 Oe = f3(dot_rn(U, O), dot_rn(V, O), dot_rn(W, O));
+    float3 De = f3(dot_rn(U, r.d), dot_rn(V, r.d), dot_rn(W, r.d));
+    float l = __fdiv_rn(1.f, __fsqrt_rn(dot_rn(De, De)));
+    float3 D = f3(__fmul_rn(De.x, l), __fmul_rn(De.y, l), __fmul_rn(De.z, l));
+    float b = -dot_rn(Oe, D);
+    float c = __fsub_rn(dot_rn(Oe, Oe), 1.f);
+    float3 p = f3(__fadd_rn(Oe.x, __fmul_rn(D.x, b)), __fadd_rn(Oe.y, __fmul_rn(D.y, b)),
+                  __fadd_rn(Oe.z, __fmul_rn(D.z, b)));
+    float disc = __fsub_rn(1.f, dot_rn(p, p));
+    if (!(disc > 1e-7f)) return false;
+    float sd = __fsqrt_rn(disc);
+    float q = __fadd_rn(b, b > 0.f ? sd : -sd);
+    root1 = __fmul_rn(__fdiv_rn(c, q), l);
+    root2 = __fmul_rn(q, l);
+    return true;
+}
+
+// The same interval from the sampling conic scaled by the threshold factor k (fast arithmetic).
+__device__ __forceinline__ bool roots_fast(const LeafRec& rec, const RayState& r, float& root1, float& root2) {
+    float3 O = r.o - f3(rec.a.x, rec.a.y, rec.a.z);
+    float k = rec.r0.w;
+    float3 r0 = f3(rec.r0.x, rec.r0.y, rec.r0.z), r1 = f3(rec.r1.x, rec.r1.y, rec.r1.z),
+           r2 = f3(rec.r2.x, rec.r2.y, rec.r2.z);
+    float3 Oe = f3(dot3(r0, O) * k, dot3(r1, O) * k, dot3(r2, O) * k);
+    float3 De = f3(dot3(r0, r.d) * k, dot3(r1, r.d) * k, dot3(r2, r.d) * k);
+    float l = 1.f / sqrtf(dot3(De, De));
+    float3 Dn = De * l;
+    float b = -dot3(Oe, Dn);
+    float c = dot3(Oe, Oe) - 1.f;
+    float3 p = Oe + Dn * b;
+    float disc = 1.f - dot3(p, p);
+    if (!(disc > 1e-7f)) return false;
+    float sd = sqrtf(disc);
+    float q = b + (b > 0.f ? sd : -sd);
+    root1 = (c / q) * l;
+    root2 = q * l;
+    return true;
+}
+
+__device__ __forceinline__ LeafIS load_is(const LeafIS* p, int i) {
+    const float4* q = reinterpret_cast<const float4*>(p + i);
+    LeafIS s;
+    s.u = __ldg(q);
+    s.v = __ldg(q + 1);
+    s.w = __ldg(q + 2);
+    return s;
+}
+
+// The reference's per-slab test for the slab starting at r.tb (exact; used at the ends of the
+// conservative ranges of long chunks in the parity arithmetic).
+__device__ __forceinline__ bool slab_hit_exact(const RenderArgs& a, int leaf, float3 mu, const RayState& r) {
+    float root1, root2;
+    if (!roots_exact(load_is(a.is_rec, leaf), mu, r, root1, root2)) return false;
+    float th = fminf(r.texit, r.tb + kSlab);
+    return th > r.tenter && fmaxf(r.tb, root1) <= fminf(th, root2);
+}
+
+// Slab range [lo, hi] of the chunk (K slabs from r.tb) hit by the interval [root1, root2].
+__device__ __forceinline__ void slab_range(const RayState& r, int K, int nv, float seg_hi, float root1, float root2,
+                                           int& lo, int& hi) {
+    lo = 255;
+    hi = -1;
+    if (K <= kExactChunk) {
+        // exact: the reference's per-slab test max(tmin, root1) <= min(tmax, root2)
+        float t = r.tb;
+#pragma unroll
+        for (int kk = 0; kk < kExactChunk; ++kk) {
+            if (kk < nv) {
+                float tn = t + kSlab;
+                float th = fminf(r.texit, tn);
+                if (th > r.tenter && fmaxf(t, root1) <= fminf(th, root2)) {
+                    lo = min(lo, kk);
+                    hi = kk;
+                }
+                t = tn;
+            }
+        }
+    } else if (fmaxf(r.tb, root1) <= fminf(seg_hi, root2)) {
+        float a = fmaxf((root1 - r.tb) * kInvSlab, -1.f);
+        float b = fminf((root2 - r.tb) * kInvSlab, 4096.f);
+        lo = max(0, (int)floorf(a) - 1);
+        hi = min(K - 1, (int)floorf(b) + 1);
+        if (lo > hi) { lo = 255; hi = -1; }
+    }
+}
+
+// Union occupancy of the chunk's slabs (256 bits): bit k set when some lane has a hit in slab k.
+__device__ __forceinline__ void occ_set(unsigned long long* occ, int lo, int hi) {
+#pragma unroll
+    for (int w = 0; w < 4; ++w) {
+        int a0 = max(lo, 64 * w), b0 = min(hi, 64 * w + 63);
+        if (a0 <= b0) {
+            int n = b0 - a0 + 1;
+            unsigned long long m = (n == 64) ? ~0ull : (((1ull << n) - 1ull) << (a0 - 64 * w));
+            occ[w] |= m;
+        }
+    }
+}
+__device__ __forceinline__ bool occ_test(const unsigned long long* occ, int k) {
+    return (occ[k >> 6] >> (k & 63)) & 1ull;
+}
+// first occupied slab >= k (K when none)
+__device__ __forceinline__ int occ_next(const unsigned long long* occ, int k, int K) {
+    for (int w = k >> 6; w < 4 && 64 * w < K; ++w) {
+        unsigned long long m = occ[w];
+        if (w == (k >> 6)) m &= (~0ull) << (k & 63);
+        if (m) return min(K, 64 * w + __ffsll((long long)m) - 1);
+    }
+    return K;
+}
+
 // Warp-cooperative traversal for the chunk [tb, seg_hi] of every active lane.  Appends hit leaves
 // with index > cursor to the warp list; returns the entry count.  `ovf` is set when the list
 // filled up before the traversal finished.
-template <int CAP>
+template <bool FAST, int CAP>
 __device__ int traverse(WarpSmem<CAP>& sm, const RenderArgs& a, const RayState& r, bool on, float seg_hi,
                         int K, int nv, int cursor, bool& ovf, int lane) {
     int count = 0;
     ovf = false;
+    unsigned long long occ[4] = {0ull, 0ull, 0ull, 0ull};
     int sp = 0;
     int cur = (a.n_leaves == 1) ? ~0 : 0;
     long long guard = 0;
@@ -111,49 +256,32 @@ __device__ int traverse(WarpSmem<CAP>& sm, const RenderArgs& a, const RayState& 
         } else {
             int leaf = ~cur;
             if (leaf > cursor) {
-                LeafRec rec = load_rec(a.rec, leaf);
-                unsigned m = 0;
+                int lo = 255, hi = -1;
                 if (on) {
-                    // exact interval against the threshold ellipsoid (reference IS program)
-                    float3 O = r.o - f3(rec.a.x, rec.a.y, rec.a.z);
-                    float k = rec.r0.w;
-                    float3 r0 = f3(rec.r0.x, rec.r0.y, rec.r0.z), r1 = f3(rec.r1.x, rec.r1.y, rec.r1.z),
-                           r2 = f3(rec.r2.x, rec.r2.y, rec.r2.z);
-                    float3 Oe = f3(dot3(r0, O) * k, dot3(r1, O) * k, dot3(r2, O) * k);
-                    float3 De = f3(dot3(r0, r.d) * k, dot3(r1, r.d) * k, dot3(r2, r.d) * k);
-                    float l = 1.f / sqrtf(dot3(De, De));
-                    float3 Dn = De * l;
-                    float b = -dot3(Oe, Dn);
-                    float c = dot3(Oe, Oe) - 1.f;
-                    float3 p = Oe + Dn * b;
-                    float disc = 1.f - dot3(p, p);
-                    if (disc > 1e-7f) {
-                        float sd = sqrtf(disc);
-                        float q = b + (b > 0.f ? sd : -sd);
-                        float root1 = (c / q) * l, root2 = q * l;
-                        float t = r.tb;
-#pragma unroll
-                        for (int kk = 0; kk < kMaxChunk; ++kk) {
-                            if (kk < nv) {
-                                float tn = t + kSlab;
-                                float hi = fminf(r.texit, tn);
-                                if (hi > r.tenter && fmaxf(t, root1) <= fminf(hi, root2)) m |= 1u << kk;
-                                t = tn;
-                            }
-                        }
+                    float root1, root2;
+                    bool ok;
+                    if (FAST) {
+                        ok = roots_fast(load_rec(a.rec, leaf), r, root1, root2);
+                    } else {
+                        float4 m4 = __ldg(reinterpret_cast<const float4*>(a.rec + leaf));
+                        ok = roots_exact(load_is(a.is_rec, leaf), f3(m4.x, m4.y, m4.z), r, root1, root2);
                     }
+                    if (ok) slab_range(r, K, nv, seg_hi, root1, root2, lo, hi);
                 }
-                unsigned any = __ballot_sync(kFull, m != 0u);
+                unsigned any = __ballot_sync(kFull, lo <= hi);
                 if (any) {
                     if (count == CAP) {
                         ovf = true;
                         break;
                     }
-                    if (lane == 0) sm.ids[count] = leaf;
-                    for (int kk = 0; kk < K; ++kk) {
-                        unsigned wk = __ballot_sync(kFull, (m >> kk) & 1u);
-                        if (lane == kk) sm.mask[kk][count] = wk;
+                    int ulo = (int)__reduce_min_sync(kFull, (unsigned)lo);
+                    int uhi = (int)__reduce_max_sync(kFull, (unsigned)(hi + 1)) - 1;
+                    sm.lrng[count][lane] = (unsigned short)((lo & 0xff) | ((hi & 0xff) << 8));
+                    if (lane == 0) {
+                        sm.ids[count] = leaf;
+                        sm.urng[count] = (unsigned)ulo | ((unsigned)uhi << 16);
                     }
+                    occ_set(occ, ulo, uhi);
                     ++count;
                 }
             }
@@ -161,6 +289,25 @@ __device__ int traverse(WarpSmem<CAP>& sm, const RenderArgs& a, const RayState& 
         if (sp == 0) break;
         __syncwarp();
         cur = sm.stack[--sp];
+    }
+    __syncwarp();
+    if (lane == 0) {
+#pragma unroll
+        for (int w = 0; w < 4; ++w) sm.occ[w] = occ[w];
+    }
+    // per-slab entry masks: lane l fills slabs l, l+32, ...
+    for (int k = lane; k < K; k += 32) {
+#pragma unroll
+        for (int w = 0; w < CAP / 32; ++w) {
+            unsigned mw = 0u;
+            const int e0 = 32 * w, e1 = min(count, e0 + 32);
+#pragma unroll 1
+            for (int e = e0; e < e1; ++e) {
+                unsigned u = sm.urng[e];
+                if (k >= (int)(u & 0xffff) && k <= (int)(u >> 16)) mw |= 1u << (e - e0);
+            }
+            sm.smask[k][w] = mw;
+        }
     }
     __syncwarp();
     return count;
@@ -179,25 +326,74 @@ __device__ __forceinline__ unsigned slab_offsets(int rnd_sample, unsigned seed, 
     return seed;
 }
 
+// Reference-order evaluation of one sample's weight with an exact threshold decision.
+__device__ __forceinline__ float parity_weight(float3 o, float3 d, float t, float3 mu, float3 r0, float3 r1,
+                                               float3 r2, float dn, float3& v, float3& m, bool& in) {
+    float3 x = f3(__fadd_rn(o.x, __fmul_rn(d.x, t)), __fadd_rn(o.y, __fmul_rn(d.y, t)),
+                  __fadd_rn(o.z, __fmul_rn(d.z, t)));
+    v = f3(__fsub_rn(x.x, mu.x), __fsub_rn(x.y, mu.y), __fsub_rn(x.z, mu.z));
+    m = rows_rn(r0, r1, r2, v);
+    float power = __fmul_rn(-0.5f, dot_rn(m, m));
+    float w = expf(power);
+    float dw = __fmul_rn(dn, w);
+    if (fabsf(dw - kSigThr) < 4e-8f) {
+        // within the exponential's error of the threshold: decide with a correctly rounded weight
+        w = (float)exp((double)power);
+        dw = __fmul_rn(dn, w);
+    }
+    in = dw > kSigThr;
+    return w;
+}
+
+__device__ __forceinline__ float parity_time(float tb, int i, int rnd_sample, const float* roff) {
+    float t = __fadd_rn(tb, __fmul_rn((float)i, kDt));
+    if (rnd_sample) t = __fadd_rn(t, roff[i]);
+    return t;
+}
+
+__device__ __forceinline__ bool in_range(unsigned short rg, int k) {
+    return k >= (int)(rg & 0xff) && k <= (int)(rg >> 8);
+}
+__device__ __forceinline__ bool in_urange(unsigned u, int k) {
+    return k >= (int)(u & 0xffff) && k <= (int)(u >> 16);
+}
+
+// Sample buffers of slab k: sum of density and density-weighted colour of the lane's hits.
+// Whether lane-entry range rg holds slab k.  Chunks longer than kExactChunk carry conservative
+// ranges; in the parity arithmetic the two slabs at each end are decided by the reference's exact
+// per-slab test (the extra slabs' samples lie outside the threshold ellipsoid, but only up to the
+// rounding of the intersection arithmetic).
+template <bool FAST>
+__device__ __forceinline__ bool lane_has_entry(const RenderArgs& a, unsigned short rg, int k, int K, int leaf,
+                                               const RayState& r) {
+    int lo = rg & 0xff, hi = rg >> 8;
+    if (k < lo || k > hi) return false;
+    if (FAST || K <= kExactChunk || (k > lo + 1 && k < hi - 1)) return true;
+    float4 m4 = __ldg(reinterpret_cast<const float4*>(a.rec + leaf));
+    return slab_hit_exact(a, leaf, f3(m4.x, m4.y, m4.z), r);
+}
+
 // Sample buffers of slab k: sum of density and density-weighted colour of the lane's hits.
 template <bool FAST, int CAP>
-__device__ __forceinline__ int slab_buffers(const WarpSmem<CAP>& sm, int count, int k, bool has, const RayState& r,
+__device__ __forceinline__ int slab_buffers(const WarpSmem<CAP>& sm, int k, int K, bool has, const RayState& r,
                                             const RenderArgs& a, long long rgb_base, const float* roff,
                                             float* sig, float3* C, int lane) {
     int nh = 0;
-    const unsigned bit = 1u << lane;
-    for (int e = 0; e < count; ++e) {
-        unsigned w = sm.mask[k][e];
-        if (w == 0u) continue;
-        if (has && (w & bit)) {
-            int leaf = sm.ids[e];
+#pragma unroll 1
+    for (int w = 0; w < CAP / 32; ++w) {
+        unsigned mw = sm.smask[k][w];
+        while (mw) {
+            const int e = 32 * w + __ffs(mw) - 1;
+            mw &= mw - 1u;
+            if (!has) continue;
+            const int leaf = sm.ids[e];
+            if (!lane_has_entry<FAST>(a, sm.lrng[e][lane], k, K, leaf, r)) continue;
             LeafRec rec = load_rec(a.rec, leaf);
             float4 col4 = __ldg(a.rgb + rgb_base + leaf);
             float3 mu = f3(rec.a.x, rec.a.y, rec.a.z);
             float dn = rec.a.w;
             float3 r0 = f3(rec.r0.x, rec.r0.y, rec.r0.z), r1 = f3(rec.r1.x, rec.r1.y, rec.r1.z),
                    r2 = f3(rec.r2.x, rec.r2.y, rec.r2.z);
-            float3 col = f3(col4.x, col4.y, col4.z);
             ++nh;
             if (FAST) {
                 float3 v0 = (r.o + r.d * r.tb) - mu;
@@ -205,6 +401,7 @@ __device__ __forceinline__ int slab_buffers(const WarpSmem<CAP>& sm, int count, 
                 float3 m0 = f3(dot3(r0, v0), dot3(r1, v0), dot3(r2, v0));
                 float3 mb = f3(dot3(r0, vb), dot3(r1, vb), dot3(r2, vb));
                 float A = dot3(m0, m0), B2 = 2.f * dot3(m0, mb), Cq = dot3(mb, mb);
+                float3 col = f3(col4.x, col4.y, col4.z);
 #pragma unroll
                 for (int i = 0; i < kBuf; ++i) {
                     float fi = (float)i;
@@ -218,14 +415,15 @@ __device__ __forceinline__ int slab_buffers(const WarpSmem<CAP>& sm, int count, 
             } else {
 #pragma unroll
                 for (int i = 0; i < kBuf; ++i) {
-                    float t = r.tb + (float)i * kDt;
-                    if (a.rnd_sample) t += roff[i];
-                    float3 v = (r.o + r.d * t) - mu;
-                    float3 m = f3(dot3(r0, v), dot3(r1, v), dot3(r2, v));
-                    float w = expf(-0.5f * dot3(m, m));
-                    if (dn * w > kSigThr) {
-                        sig[i] += dn * w;
-                        C[i] = C[i] + (col * w) * dn;
+                    float t = parity_time(r.tb, i, a.rnd_sample, roff);
+                    float3 v, m;
+                    bool in;
+                    float w = parity_weight(r.o, r.d, t, mu, r0, r1, r2, dn, v, m, in);
+                    if (in) {
+                        sig[i] = __fadd_rn(sig[i], __fmul_rn(dn, w));
+                        C[i] = f3(__fadd_rn(C[i].x, __fmul_rn(__fmul_rn(col4.x, w), dn)),
+                                  __fadd_rn(C[i].y, __fmul_rn(__fmul_rn(col4.y, w), dn)),
+                                  __fadd_rn(C[i].z, __fmul_rn(__fmul_rn(col4.z, w), dn)));
                     }
                 }
             }
@@ -236,19 +434,31 @@ __device__ __forceinline__ int slab_buffers(const WarpSmem<CAP>& sm, int count, 
 
 template <bool FAST>
 __device__ __forceinline__ float exp_neg(float x) {
-    // exp(-x) for the compositing alpha
-    return FAST ? ex2_approx(-x * 1.4426950408889634f) : expf(-x);
+    return FAST ? ex2_approx(-x * 1.4426950408889634f) : (float)exp(-(double)x);
 }
 
 template <bool FAST>
 __device__ __forceinline__ void composite(RayState& r, const float* sig, const float3* C) {
 #pragma unroll
     for (int i = 0; i < kBuf; ++i) {
-        float alpha = 1.f - exp_neg<FAST>(sig[i] * kDt);
-        float3 c = C[i];
-        if (sig[i] > 0.f) c = c * (1.f / sig[i]);
-        r.C = r.C + c * (r.T * alpha);
-        r.T *= 1.f - alpha;
+        if (FAST) {
+            float alpha = 1.f - exp_neg<true>(sig[i] * kDt);
+            float3 c = C[i];
+            if (sig[i] > 0.f) c = c * (1.f / sig[i]);
+            r.C = r.C + c * (r.T * alpha);
+            r.T *= 1.f - alpha;
+        } else {
+            float alpha = __fsub_rn(1.f, exp_neg<false>(__fmul_rn(sig[i], kDt)));
+            float3 c = C[i];
+            if (sig[i] > 0.f) {
+                float inv = __fdiv_rn(1.f, sig[i]);
+                c = f3(__fmul_rn(c.x, inv), __fmul_rn(c.y, inv), __fmul_rn(c.z, inv));
+            }
+            float ta = __fmul_rn(r.T, alpha);
+            r.C = f3(__fadd_rn(r.C.x, __fmul_rn(c.x, ta)), __fadd_rn(r.C.y, __fmul_rn(c.y, ta)),
+                     __fadd_rn(r.C.z, __fmul_rn(c.z, ta)));
+            r.T = __fmul_rn(r.T, __fsub_rn(1.f, alpha));
+        }
     }
 }
 
@@ -263,23 +473,60 @@ __device__ __forceinline__ float4 quat_grad(float4 q, float3 d1, float3 d2, floa
     return o;
 }
 
+// Transposed warp reduction of 16 values: afterwards lane l holds the warp sum of value
+// 8*b4 + 4*b3 + 2*b2 + b1 (b_i = bit i of l); lanes l and l^1 hold the same value.
+__device__ __forceinline__ float transpose_reduce16(float* v, int lane) {
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+        bool up = lane & 16;
+        float send = up ? v[i] : v[i + 8];
+        float keep = up ? v[i + 8] : v[i];
+        v[i] = keep + __shfl_xor_sync(kFull, send, 16);
+    }
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+        bool up = lane & 8;
+        float send = up ? v[i] : v[i + 4];
+        float keep = up ? v[i + 4] : v[i];
+        v[i] = keep + __shfl_xor_sync(kFull, send, 8);
+    }
+#pragma unroll
+    for (int i = 0; i < 2; ++i) {
+        bool up = lane & 4;
+        float send = up ? v[i] : v[i + 2];
+        float keep = up ? v[i + 2] : v[i];
+        v[i] = keep + __shfl_xor_sync(kFull, send, 4);
+    }
+    {
+        bool up = lane & 2;
+        float send = up ? v[0] : v[1];
+        float keep = up ? v[1] : v[0];
+        v[0] = keep + __shfl_xor_sync(kFull, send, 2);
+    }
+    v[0] += __shfl_xor_sync(kFull, v[0], 1);
+    return v[0];
+}
+
 // Adjoint of slab k for all list entries: per-lane gradient of each hit Gaussian, warp reduction,
-// one set of vector atomics per entry.
+// one atomic per value.  Value order: ddens, dpos.xyz, dscale.xyz, dquat.xyzw, drgb.xyz.
 template <bool FAST, int CAP>
-__device__ __forceinline__ void slab_adjoint(const WarpSmem<CAP>& sm, int count, int k, bool has, const RayState& r,
-                                             const RenderArgs& a, int view, long long rgb_base, const float* roff,
+__device__ __forceinline__ void slab_adjoint(const WarpSmem<CAP>& sm, int k, int K, bool has, const RayState& r,
+                                             const RenderArgs& a, long long rgb_base, const float* roff,
                                              const float* E, const float* F, const float* G, int lane) {
-    const unsigned bit = 1u << lane;
-    for (int e = 0; e < count; ++e) {
-        unsigned w = sm.mask[k][e];
-        if (w == 0u) continue;
-        bool act = has && (w & bit);
+    const int vid = ((lane >> 4) & 1) * 8 + ((lane >> 3) & 1) * 4 + ((lane >> 2) & 1) * 2 + ((lane >> 1) & 1);
+#pragma unroll 1
+    for (int w = 0; w < CAP / 32; ++w) {
+      unsigned mw = sm.smask[k][w];
+      while (mw) {
+        const int e = 32 * w + __ffs(mw) - 1;
+        mw &= mw - 1u;
+        const int leaf = sm.ids[e];
+        bool act = has && lane_has_entry<FAST>(a, sm.lrng[e][lane], k, K, leaf, r);
         unsigned am = __ballot_sync(kFull, act);
         if (am == 0u) continue;
-        int leaf = sm.ids[e];
-        float v[14];
+        float v[16];
 #pragma unroll
-        for (int z = 0; z < 14; ++z) v[z] = 0.f;
+        for (int z = 0; z < 16; ++z) v[z] = 0.f;
         if (act) {
             LeafRec rec = load_rec(a.rec, leaf);
             float4 col4 = __ldg(a.rgb + rgb_base + leaf);
@@ -334,12 +581,11 @@ __device__ __forceinline__ void slab_adjoint(const WarpSmem<CAP>& sm, int count,
             } else {
 #pragma unroll
                 for (int i = 0; i < kBuf; ++i) {
-                    float t = r.tb + (float)i * kDt;
-                    if (a.rnd_sample) t += roff[i];
-                    float3 vv = (r.o + r.d * t) - mu;
-                    float3 m = f3(dot3(r0, vv), dot3(r1, vv), dot3(r2, vv));
-                    float wt = expf(-0.5f * dot3(m, m));
-                    if (dn * wt > kSigThr) {
+                    float t = parity_time(r.tb, i, a.rnd_sample, roff);
+                    float3 vv, m;
+                    bool in;
+                    float wt = parity_weight(r.o, r.d, t, mu, r0, r1, r2, dn, vv, m, in);
+                    if (in) {
                         float h = E[i] + F[i] * (gcol - G[i]);
                         gc += wt * dn * F[i];
                         dd += wt * h;
@@ -362,21 +608,46 @@ __device__ __forceinline__ void slab_adjoint(const WarpSmem<CAP>& sm, int count,
             v[7] = dq.x; v[8] = dq.y; v[9] = dq.z; v[10] = dq.w;
             v[11] = r.g.x * gc; v[12] = r.g.y * gc; v[13] = r.g.z * gc;
         }
-        int leader = __ffs(am) - 1;
-        if (__popc(am) > 1) {
-#pragma unroll
-            for (int z = 0; z < 14; ++z) {
-#pragma unroll
-                for (int o = 16; o; o >>= 1) v[z] += __shfl_xor_sync(kFull, v[z], o);
+        float* gg = reinterpret_cast<float*>(a.gacc_geo + 3 * (long long)leaf);
+        float* gr = reinterpret_cast<float*>(a.gacc_rgb + rgb_base + leaf);
+        if (__popc(am) == 1) {
+            if (act) {
+                float4* g4 = reinterpret_cast<float4*>(gg);
+                atomicAdd(g4, make_float4(v[0], v[1], v[2], v[3]));
+                atomicAdd(g4 + 1, make_float4(v[4], v[5], v[6], v[7]));
+                atomicAdd(g4 + 2, make_float4(v[8], v[9], v[10], 0.f));
+                atomicAdd(reinterpret_cast<float4*>(gr), make_float4(v[11], v[12], v[13], 0.f));
+            }
+        } else {
+            float s = transpose_reduce16(v, lane);
+            if (!(lane & 1) && vid < 14) {
+                if (vid < 11) atomicAdd(gg + vid, s);
+                else atomicAdd(gr + (vid - 11), s);
             }
         }
-        if (lane == leader) {
-            float4* gg = a.gacc_geo + 3 * (long long)leaf;
-            atomicAdd(gg, make_float4(v[0], v[1], v[2], v[3]));
-            atomicAdd(gg + 1, make_float4(v[4], v[5], v[6], 0.f));
-            atomicAdd(gg + 2, make_float4(v[7], v[8], v[9], v[10]));
-            atomicAdd(a.gacc_rgb + rgb_base + leaf, make_float4(v[11], v[12], v[13], 0.f));
-        }
+      }
+    }
+}
+
+// Per-sample compositing adjoint scalars of one slab (reference backward :675-730):
+// E = g.((T c - R) dt), F = T alpha / sigma, G = g.c ; advances T and R over the slab.
+template <bool FAST>
+__device__ __forceinline__ void slab_adjoint_scalars(const RayState& r, const float* sig, const float3* Cb, float* E,
+                                                     float* F, float* G, float& Ta, float3& Ra) {
+    Ta = r.T;
+    Ra = r.C;
+#pragma unroll
+    for (int i = 0; i < kBuf; ++i) {
+        float cd = sig[i];
+        float3 cc = Cb[i];
+        if (cd > 0.f) cc = cc * (1.f / cd);
+        float alpha = FAST ? 1.f - exp_neg<true>(cd * kDt) : __fsub_rn(1.f, exp_neg<false>(__fmul_rn(cd, kDt)));
+        float3 aux = (cc * Ta - Ra) * kDt;
+        E[i] = dot3(r.g, aux);
+        F[i] = cd > 0.f ? Ta * alpha / cd : 0.f;
+        G[i] = dot3(r.g, cc);
+        Ra = Ra - cc * (Ta * alpha);
+        Ta = FAST ? Ta * (1.f - alpha) : __fmul_rn(Ta, __fsub_rn(1.f, alpha));
     }
 }
 
@@ -391,6 +662,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32) k_render(RenderArgs a) {
 #pragma unroll
     for (int z = 0; z < 6; ++z) scene[z] = ord2f(a.scene_ord[z]);
     unsigned long long hits_acc = 0, slabs_acc = 0;
+    const int kmax = min((a.rnd_sample == 1) ? min(a.chunk_slabs, kExactChunk) : a.chunk_slabs, kMaskChunk);
 
     while (true) {
         int tile = 0;
@@ -418,28 +690,30 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32) k_render(RenderArgs a) {
         RayState r;
         r.seed = tea4(a.iteration, ray_l);
         {
+            // computeRay (forward/gaussians_aabb.cu:405-434) in IEEE operation order
             float ix, iy;
             if (a.jitter == 1) {
                 float jx = lcg_rnd(r.seed) * 0.333333f;
                 float jy = lcg_rnd(r.seed) * 0.333333f;
-                ix = ((float)(ray_l % (unsigned)W) + 0.333333f + jx) / (float)W;
-                iy = ((float)(ray_l / (unsigned)W) + 0.333333f + jy) / (float)H;
+                ix = __fdiv_rn(__fadd_rn(__fadd_rn((float)(ray_l % (unsigned)W), 0.333333f), jx), (float)W);
+                iy = __fdiv_rn(__fadd_rn(__fadd_rn((float)(ray_l / (unsigned)W), 0.333333f), jy), (float)H);
             } else {
-                ix = ((float)(ray_l % (unsigned)W) + 0.5f) / (float)W;
-                iy = ((float)(ray_l / (unsigned)W) + 0.5f) / (float)H;
+                ix = __fdiv_rn(__fadd_rn((float)(ray_l % (unsigned)W), 0.5f), (float)W);
+                iy = __fdiv_rn(__fadd_rn((float)(ray_l / (unsigned)W), 0.5f), (float)H);
             }
-            float dx = (2.f * ix - 1.f) * cam.tan_half_fovx;
-            float dy = (2.f * iy - 1.f) * cam.tan_half_fovy;
-            float3 dir = f3(dx * cam.u[0] + dy * cam.v[0] + cam.w[0], dx * cam.u[1] + dy * cam.v[1] + cam.w[1],
-                            dx * cam.u[2] + dy * cam.v[2] + cam.w[2]);
-            float inv = 1.f / sqrtf(dot3(dir, dir));
-            r.d = dir * inv;
+            float dx = __fmul_rn(__fsub_rn(__fmul_rn(2.f, ix), 1.f), cam.tan_half_fovx);
+            float dy = __fmul_rn(__fsub_rn(__fmul_rn(2.f, iy), 1.f), cam.tan_half_fovy);
+            float3 dir = f3(__fadd_rn(__fadd_rn(__fmul_rn(cam.u[0], dx), __fmul_rn(cam.v[0], dy)), cam.w[0]),
+                            __fadd_rn(__fadd_rn(__fmul_rn(cam.u[1], dx), __fmul_rn(cam.v[1], dy)), cam.w[1]),
+                            __fadd_rn(__fadd_rn(__fmul_rn(cam.u[2], dx), __fmul_rn(cam.v[2], dy)), cam.w[2]));
+            float inv = __fdiv_rn(1.f, __fsqrt_rn(dot_rn(dir, dir)));
+            r.d = f3(__fmul_rn(dir.x, inv), __fmul_rn(dir.y, inv), __fmul_rn(dir.z, inv));
             r.o = f3(cam.eye[0], cam.eye[1], cam.eye[2]);
         }
         {
-            float t0x = (scene[0] - r.o.x) / r.d.x, t1x = (scene[3] - r.o.x) / r.d.x;
-            float t0y = (scene[1] - r.o.y) / r.d.y, t1y = (scene[4] - r.o.y) / r.d.y;
-            float t0z = (scene[2] - r.o.z) / r.d.z, t1z = (scene[5] - r.o.z) / r.d.z;
+            float t0x = __fdiv_rn(scene[0] - r.o.x, r.d.x), t1x = __fdiv_rn(scene[3] - r.o.x, r.d.x);
+            float t0y = __fdiv_rn(scene[1] - r.o.y, r.d.y), t1y = __fdiv_rn(scene[4] - r.o.y, r.d.y);
+            float t0z = __fdiv_rn(scene[2] - r.o.z, r.d.z), t1z = __fdiv_rn(scene[5] - r.o.z, r.d.z);
             r.tenter = fmaxf(0.f, fmaxf(fminf(t0x, t1x), fmaxf(fminf(t0y, t1y), fminf(t0z, t1z))));
             r.texit = fminf(fmaxf(t0x, t1x), fminf(fmaxf(t0y, t1y), fmaxf(t0z, t1z)));
         }
@@ -452,20 +726,14 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32) k_render(RenderArgs a) {
         r.alive = valid && (r.tenter < r.texit);
         r.tb = r.tenter;
         r.T = 1.f;
-        if (BWD) {
-            if (valid) {
-                r.C = f3(a.ray_colors_in[3 * ray_g], a.ray_colors_in[3 * ray_g + 1], a.ray_colors_in[3 * ray_g + 2]);
-                r.g = f3(a.dL[3 * ray_g], a.dL[3 * ray_g + 1], a.dL[3 * ray_g + 2]);
-            } else {
-                r.C = f3(0.f, 0.f, 0.f);
-                r.g = f3(0.f, 0.f, 0.f);
-            }
-        } else {
-            r.C = f3(0.f, 0.f, 0.f);
-            r.g = f3(0.f, 0.f, 0.f);
+        r.C = f3(0.f, 0.f, 0.f);
+        r.g = f3(0.f, 0.f, 0.f);
+        if (BWD && valid) {
+            r.C = f3(a.ray_colors_in[3 * ray_g], a.ray_colors_in[3 * ray_g + 1], a.ray_colors_in[3 * ray_g + 2]);
+            r.g = f3(a.dL[3 * ray_g], a.dL[3 * ray_g + 1], a.dL[3 * ray_g + 2]);
         }
 
-        int K = a.chunk_slabs;
+        int K = min(kExactChunk, kmax);
         int rounds = 0;
         while (true) {
             bool on = r.alive;
@@ -478,16 +746,22 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32) k_render(RenderArgs a) {
             int nv = 0;
             float seg_hi = r.tb;
             if (on) {
-                float t = r.tb;
-                for (int kk = 0; kk < K; ++kk) {
-                    if (t < r.texit) { nv = kk + 1; t = t + kSlab; } else break;
+                if (K <= kExactChunk) {
+                    float t = r.tb;
+                    for (int kk = 0; kk < K; ++kk) {
+                        if (t < r.texit) { nv = kk + 1; t = t + kSlab; } else break;
+                    }
+                    seg_hi = fminf(r.texit, t);
+                } else {
+                    nv = K;
+                    seg_hi = fminf(r.texit, r.tb + (float)(K + 1) * kSlab);
                 }
-                seg_hi = fminf(r.texit, t);
                 // a slab step that no longer changes tb (|t| beyond ~2^19) would march forever
-                if (nv == 0 || r.tb + kSlab == r.tb) { r.alive = false; on = false; nv = 0; }
+                if (!(r.tb < r.texit) || r.tb + kSlab == r.tb) { r.alive = false; on = false; nv = 0; }
             }
             bool ovf;
-            int count = traverse<CAP>(sm, a, r, on, seg_hi, K, nv, -1, ovf, lane);
+            int count = traverse<FAST, CAP>(sm, a, r, on, seg_hi, K, nv, -1, ovf, lane);
+            const unsigned long long* occ = sm.occ;
             if (ovf && K > 1) {
                 K = max(1, K >> 1);
                 if (lane == 0) atomicAdd(&a.st->chunk_splits, 1ull);
@@ -495,14 +769,27 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32) k_render(RenderArgs a) {
             }
             if (!ovf) {
                 for (int k = 0; k < K; ++k) {
-                    bool has = on && k < nv && r.T > kTeps;
+                    bool has = on && r.tb < r.texit && r.T > kTeps;
+                    if (!__any_sync(kFull, has)) break;
+                    if (!occ_test(occ, k)) {
+                        // no lane has a hit in slabs [k, k2): march them (tb only; T is unchanged)
+                        int k2 = occ_next(occ, k, K);
+                        if (has) {
+                            for (int j = k; j < k2 && r.tb < r.texit; ++j) {
+                                r.tb = r.tb + kSlab;
+                                ++slabs_acc;
+                            }
+                        }
+                        k = k2 - 1;
+                        continue;
+                    }
                     float roff[kBuf];
                     unsigned seed_next = slab_offsets(a.rnd_sample, r.seed, roff);
                     float sig[kBuf];
                     float3 Cb[kBuf];
 #pragma unroll
                     for (int i = 0; i < kBuf; ++i) { sig[i] = 0.f; Cb[i] = f3(0.f, 0.f, 0.f); }
-                    int nh = slab_buffers<FAST, CAP>(sm, count, k, has, r, a, rgb_base, roff, sig, Cb, lane);
+                    int nh = slab_buffers<FAST, CAP>(sm, k, K, has, r, a, rgb_base, roff, sig, Cb, lane);
                     if (has) {
                         ++slabs_acc;
                         hits_acc += nh;
@@ -514,24 +801,11 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32) k_render(RenderArgs a) {
                             r.seed = seed_next;
                         }
                     } else {
-                        float E[kBuf], F[kBuf], G[kBuf];
-                        float Ta = r.T;
-                        float3 Ra = r.C;
-#pragma unroll
-                        for (int i = 0; i < kBuf; ++i) {
-                            float cd = sig[i];
-                            float3 cc = Cb[i];
-                            if (cd > 0.f) cc = cc * (1.f / cd);
-                            float alpha = 1.f - exp_neg<FAST>(cd * kDt);
-                            float3 aux = (cc * Ta - Ra) * kDt;
-                            E[i] = dot3(r.g, aux);
-                            F[i] = cd > 0.f ? Ta * alpha / cd : 0.f;
-                            G[i] = dot3(r.g, cc);
-                            Ra = Ra - cc * (Ta * alpha);
-                            Ta *= 1.f - alpha;
-                        }
+                        float E[kBuf], F[kBuf], G[kBuf], Ta;
+                        float3 Ra;
+                        slab_adjoint_scalars<FAST>(r, sig, Cb, E, F, G, Ta, Ra);
                         bool act = has && nh > 0;
-                        slab_adjoint<FAST, CAP>(sm, count, k, act, r, a, view, rgb_base, roff, E, F, G, lane);
+                        slab_adjoint<FAST, CAP>(sm, k, K, act, r, a, rgb_base, roff, E, F, G, lane);
                         if (act) {
                             r.T = Ta;
                             r.C = Ra;
@@ -540,7 +814,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32) k_render(RenderArgs a) {
                     }
                     if (has) r.tb = r.tb + kSlab;
                 }
-                if (count < CAP / 4 && K < a.chunk_slabs) K = min(a.chunk_slabs, K << 1);
+                if (count < CAP / 4 && K < kmax) K = min(kmax, K << 1);
             } else {
                 // K == 1 and more hits than the list holds: consume the slab in several passes
                 bool has = on && nv > 0 && r.T > kTeps;
@@ -550,14 +824,14 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32) k_render(RenderArgs a) {
                 float3 Cb[kBuf];
 #pragma unroll
                 for (int i = 0; i < kBuf; ++i) { sig[i] = 0.f; Cb[i] = f3(0.f, 0.f, 0.f); }
-                int nh = slab_buffers<FAST, CAP>(sm, count, 0, has, r, a, rgb_base, roff, sig, Cb, lane);
+                int nh = slab_buffers<FAST, CAP>(sm, 0, 1, has, r, a, rgb_base, roff, sig, Cb, lane);
                 bool more = ovf;
                 while (more) {
                     int cursor = sm.ids[count - 1];
                     __syncwarp();
                     if (lane == 0) atomicAdd(&a.st->list_passes, 1ull);
-                    count = traverse<CAP>(sm, a, r, on, seg_hi, 1, nv, cursor, more, lane);
-                    nh += slab_buffers<FAST, CAP>(sm, count, 0, has, r, a, rgb_base, roff, sig, Cb, lane);
+                    count = traverse<FAST, CAP>(sm, a, r, on, seg_hi, 1, nv, cursor, more, lane);
+                    nh += slab_buffers<FAST, CAP>(sm, 0, 1, has, r, a, rgb_base, roff, sig, Cb, lane);
                 }
                 if (has) {
                     ++slabs_acc;
@@ -570,28 +844,15 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32) k_render(RenderArgs a) {
                         r.seed = seed_next;
                     }
                 } else {
-                    float E[kBuf], F[kBuf], G[kBuf];
-                    float Ta = r.T;
-                    float3 Ra = r.C;
-#pragma unroll
-                    for (int i = 0; i < kBuf; ++i) {
-                        float cd = sig[i];
-                        float3 cc = Cb[i];
-                        if (cd > 0.f) cc = cc * (1.f / cd);
-                        float alpha = 1.f - exp_neg<FAST>(cd * kDt);
-                        float3 aux = (cc * Ta - Ra) * kDt;
-                        E[i] = dot3(r.g, aux);
-                        F[i] = cd > 0.f ? Ta * alpha / cd : 0.f;
-                        G[i] = dot3(r.g, cc);
-                        Ra = Ra - cc * (Ta * alpha);
-                        Ta *= 1.f - alpha;
-                    }
+                    float E[kBuf], F[kBuf], G[kBuf], Ta;
+                    float3 Ra;
+                    slab_adjoint_scalars<FAST>(r, sig, Cb, E, F, G, Ta, Ra);
                     bool act = has && nh > 0;
                     int cursor = -1;
                     bool more2 = true;
                     while (more2) {
-                        count = traverse<CAP>(sm, a, r, on, seg_hi, 1, nv, cursor, more2, lane);
-                        slab_adjoint<FAST, CAP>(sm, count, 0, act, r, a, view, rgb_base, roff, E, F, G, lane);
+                        count = traverse<FAST, CAP>(sm, a, r, on, seg_hi, 1, nv, cursor, more2, lane);
+                        slab_adjoint<FAST, CAP>(sm, 0, 1, act, r, a, rgb_base, roff, E, F, G, lane);
                         if (more2) cursor = sm.ids[count - 1];
                         __syncwarp();
                     }
@@ -606,9 +867,9 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32) k_render(RenderArgs a) {
             if (on) r.alive = r.alive && (r.T > kTeps) && (r.tb < r.texit);
         }
         if (!BWD && valid) {
-            a.ray_colors[3 * ray_g] = r.C.x + r.T * bg;
-            a.ray_colors[3 * ray_g + 1] = r.C.y + r.T * bg;
-            a.ray_colors[3 * ray_g + 2] = r.C.z + r.T * bg;
+            a.ray_colors[3 * ray_g] = __fadd_rn(r.C.x, __fmul_rn(r.T, bg));
+            a.ray_colors[3 * ray_g + 1] = __fadd_rn(r.C.y, __fmul_rn(r.T, bg));
+            a.ray_colors[3 * ray_g + 2] = __fadd_rn(r.C.z, __fmul_rn(r.T, bg));
             if (a.final_T) a.final_T[ray_g] = r.T;
         }
     }
@@ -627,16 +888,15 @@ int render_block_threads() { return kWarpsPerBlock * 32; }
 
 size_t render_smem_bytes(bool, int cap) {
     if (cap <= 64) return sizeof(WarpSmem<64>) * kWarpsPerBlock;
-    if (cap <= 128) return sizeof(WarpSmem<128>) * kWarpsPerBlock;
-    return sizeof(WarpSmem<256>) * kWarpsPerBlock;
+    return sizeof(WarpSmem<128>) * kWarpsPerBlock;
 }
+static_assert(sizeof(WarpSmem<128>) * kWarpsPerBlock <= 48 * 1024, "static shared memory limit");
 
 template <bool BWD, bool FAST>
 static cudaError_t launch_cap(int cap, int grid, const RenderArgs& a, cudaStream_t s) {
     const int threads = kWarpsPerBlock * 32;
     if (cap <= 64) k_render<BWD, FAST, 64><<<grid, threads, 0, s>>>(a);
-    else if (cap <= 128) k_render<BWD, FAST, 128><<<grid, threads, 0, s>>>(a);
-    else k_render<BWD, FAST, 256><<<grid, threads, 0, s>>>(a);
+    else k_render<BWD, FAST, 128><<<grid, threads, 0, s>>>(a);
     return cudaGetLastError();
 }
 
@@ -645,8 +905,7 @@ static int occ_cap(int cap) {
     int nb = 0;
     const int threads = kWarpsPerBlock * 32;
     if (cap <= 64) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_render<BWD, FAST, 64>, threads, 0);
-    else if (cap <= 128) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_render<BWD, FAST, 128>, threads, 0);
-    else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_render<BWD, FAST, 256>, threads, 0);
+    else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_render<BWD, FAST, 128>, threads, 0);
     return nb;
 }
 

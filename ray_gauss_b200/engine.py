@@ -172,6 +172,11 @@ class Engine:
         check(self.lib.rg_get_status(self.h, ctypes.byref(st), int(bool(reset)), _stream()), self.h, "rg_get_status")
         return {k: int(getattr(st, k)) for k, _ in _lib.rg_status._fields_}
 
+    def leaf_order(self, n):
+        out = torch.empty((n,), dtype=torch.int32, device=self.device)
+        check(self.lib.rg_leaf_order(self.h, _ptr(out), _stream()), self.h, "rg_leaf_order")
+        return out
+
     def kernel_launches(self) -> int:
         return int(self.lib.rg_kernel_launches(self.h))
 
