@@ -131,6 +131,12 @@ typedef struct rg_status {
     uint64_t stack_overflows;          /* traversal stack overflows (result incomplete) */
     uint64_t watchdog_trips;           /* work items abandoned by the iteration limit */
     uint64_t nonfinite_inputs;         /* Gaussians with a non-finite parameter (skipped) */
+    uint64_t traversals;               /* warp-level BVH traversals (one per chunk and pass) */
+    uint64_t node_visits;              /* warp-level internal-node visits */
+    uint64_t leaf_tests;               /* warp-level leaf (exact ellipsoid) tests */
+    uint64_t list_entries;             /* warp hit-list entries appended */
+    uint64_t slab_steps;               /* warp-level slab iterations with at least one entry */
+    uint64_t entry_slabs;              /* warp-level (entry, slab) evaluations */
 } rg_status;
 
 /* Kernel tuning knobs (rg_autotune picks them; 0 = keep the current value). */

@@ -55,7 +55,8 @@ class rg_gradients(ctypes.Structure):
 class rg_status(ctypes.Structure):
     _fields_ = [(k, ctypes.c_uint64) for k in ("hit_pairs", "slabs", "slab_cap_exceeded", "list_passes",
                                                 "chunk_splits", "stack_overflows", "watchdog_trips",
-                                                "nonfinite_inputs")]
+                                                "nonfinite_inputs", "traversals", "node_visits", "leaf_tests",
+                                                "list_entries", "slab_steps", "entry_slabs")]
 
 
 class rg_tuning(ctypes.Structure):

@@ -407,6 +407,12 @@ int rg_get_status(rg_engine* e, rg_status* out, int32_t reset, void* stream) {
     out->stack_overflows = h.stack_overflows;
     out->watchdog_trips = h.watchdog_trips;
     out->nonfinite_inputs = h.nonfinite_inputs;
+    out->traversals = h.traversals;
+    out->node_visits = h.node_visits;
+    out->leaf_tests = h.leaf_tests;
+    out->list_entries = h.list_entries;
+    out->slab_steps = h.slab_steps;
+    out->entry_slabs = h.entry_slabs;
     if (reset) RG_CUDA(cudaMemset(e->st, 0, sizeof(rg::DevStatus)), "reset status");
     return RG_OK;
 }

@@ -32,6 +32,12 @@ struct DevStatus {
     unsigned long long stack_overflows;
     unsigned long long watchdog_trips;
     unsigned long long nonfinite_inputs;
+    unsigned long long traversals;        // warp-level BVH traversals
+    unsigned long long node_visits;       // warp-level internal-node visits
+    unsigned long long leaf_tests;        // warp-level leaf (ellipsoid) tests
+    unsigned long long list_entries;      // hit-list entries appended
+    unsigned long long slab_steps;        // warp-level slab iterations with at least one entry
+    unsigned long long entry_slabs;       // warp-level (entry, slab) evaluations
 };
 
 // Per-launch view table computed on the device from the camera array (no host sync).

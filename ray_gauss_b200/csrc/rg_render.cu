@@ -45,16 +45,28 @@ constexpr float kNegHalfLog2e = -0.72134752044448170f;
 constexpr float kInvSlab = 50.0f;          // 1 / 0.02
 constexpr int kExactChunk = 8;             // chunks up to this length use exact slab ranges
 
-constexpr int kMaskChunk = 128;            // longest chunk (slab entry masks are kept per slab)
-
-template <int CAP>
+// Warp hit-list layout.  Parity arithmetic keeps, per entry and lane, the exact range of the
+// chunk's slabs the lane's interval covers (64 B per entry); the fast arithmetic keeps only the mask
+// of lanes whose interval overlaps the chunk (4 B per entry) and lets those lanes evaluate every
+// slab of the entry's union range (samples outside the lane's interval fall outside the threshold
+// ellipsoid and are masked out), which allows 4x longer lists and so 4x longer chunks in dense
+// regions.
+template <bool FAST, int CAP>
 struct WarpSmem {
+    static constexpr int KM = FAST ? 64 : 128;      // longest chunk (slab entry masks per slab)
     int ids[CAP];
-    unsigned urng[CAP];                    // union of the lanes' slab ranges: lo | hi << 16
-    unsigned short lrng[CAP][32];          // per lane: lo | hi << 8 (lo > hi: not hit)
-    unsigned smask[kMaskChunk][CAP / 32];  // entries whose union range holds slab k
-    unsigned long long occ[4];             // slabs holding any entry (union occupancy)
+    unsigned urng[CAP];                              // union of the lanes' slab ranges: lo | hi << 16
+    unsigned lmask[FAST ? CAP : 1];                  // fast: lanes whose interval overlaps the chunk
+    unsigned short lrng[FAST ? 1 : CAP][32];         // parity: per lane lo | hi << 8 (lo > hi: no hit)
+    unsigned smask[KM][CAP / 32];                    // entries whose union range holds slab k
+    unsigned long long occ[4];                       // slabs holding any entry (union occupancy)
     int stack[kStack];
+};
+
+// Warp-uniform activity counters (flushed once per warp).
+struct WarpStats {
+    unsigned long long traversals = 0, node_visits = 0, leaf_tests = 0, entries = 0, slab_steps = 0,
+                       entry_slabs = 0;
 };
 
 struct RayState {
@@ -217,9 +229,10 @@ __device__ __forceinline__ int occ_next(const unsigned long long* occ, int k, in
 // with index > cursor to the warp list; returns the entry count.  `ovf` is set when the list
 // filled up before the traversal finished.
 template <bool FAST, int CAP>
-__device__ int traverse(WarpSmem<CAP>& sm, const RenderArgs& a, const RayState& r, bool on, float seg_hi,
-                        int K, int nv, int cursor, bool& ovf, int lane) {
+__device__ int traverse(WarpSmem<FAST, CAP>& sm, const RenderArgs& a, const RayState& r, bool on, float seg_hi,
+                        int K, int nv, int cursor, bool& ovf, int lane, WarpStats& ws) {
     int count = 0;
+    ++ws.traversals;
     ovf = false;
     unsigned long long occ[4] = {0ull, 0ull, 0ull, 0ull};
     int sp = 0;
@@ -232,6 +245,7 @@ __device__ int traverse(WarpSmem<CAP>& sm, const RenderArgs& a, const RayState& 
             break;
         }
         if (cur >= 0) {
+            ++ws.node_visits;
             const float4* np = reinterpret_cast<const float4*>(a.nodes + cur);
             float4 n0 = __ldg(np), n1 = __ldg(np + 1), n2 = __ldg(np + 2);
             int4 n3 = __ldg(reinterpret_cast<const int4*>(np + 3));
@@ -256,6 +270,7 @@ __device__ int traverse(WarpSmem<CAP>& sm, const RenderArgs& a, const RayState& 
         } else {
             int leaf = ~cur;
             if (leaf > cursor) {
+                ++ws.leaf_tests;
                 int lo = 255, hi = -1;
                 if (on) {
                     float root1, root2;
@@ -276,7 +291,11 @@ __device__ int traverse(WarpSmem<CAP>& sm, const RenderArgs& a, const RayState& 
                     }
                     int ulo = (int)__reduce_min_sync(kFull, (unsigned)lo);
                     int uhi = (int)__reduce_max_sync(kFull, (unsigned)(hi + 1)) - 1;
-                    sm.lrng[count][lane] = (unsigned short)((lo & 0xff) | ((hi & 0xff) << 8));
+                    if (FAST) {
+                        if (lane == 0) sm.lmask[count] = any;
+                    } else {
+                        sm.lrng[count][lane] = (unsigned short)((lo & 0xff) | ((hi & 0xff) << 8));
+                    }
                     if (lane == 0) {
                         sm.ids[count] = leaf;
                         sm.urng[count] = (unsigned)ulo | ((unsigned)uhi << 16);
@@ -295,6 +314,7 @@ __device__ int traverse(WarpSmem<CAP>& sm, const RenderArgs& a, const RayState& 
 #pragma unroll
         for (int w = 0; w < 4; ++w) sm.occ[w] = occ[w];
     }
+    ws.entries += count;
     // per-slab entry masks: lane l fills slabs l, l+32, ...
     for (int k = lane; k < K; k += 32) {
 #pragma unroll
@@ -358,26 +378,27 @@ __device__ __forceinline__ bool in_urange(unsigned u, int k) {
     return k >= (int)(u & 0xffff) && k <= (int)(u >> 16);
 }
 
-// Sample buffers of slab k: sum of density and density-weighted colour of the lane's hits.
 // Whether lane-entry range rg holds slab k.  Chunks longer than kExactChunk carry conservative
 // ranges; in the parity arithmetic the two slabs at each end are decided by the reference's exact
 // per-slab test (the extra slabs' samples lie outside the threshold ellipsoid, but only up to the
 // rounding of the intersection arithmetic).
-template <bool FAST>
-__device__ __forceinline__ bool lane_has_entry(const RenderArgs& a, unsigned short rg, int k, int K, int leaf,
-                                               const RayState& r) {
+template <bool FAST, int CAP>
+__device__ __forceinline__ bool lane_has_entry(const WarpSmem<FAST, CAP>& sm, const RenderArgs& a, int e, int k, int K,
+                                               int leaf, const RayState& r, int lane) {
+    if (FAST) return (sm.lmask[e] >> lane) & 1u;
+    unsigned short rg = sm.lrng[e][lane];
     int lo = rg & 0xff, hi = rg >> 8;
     if (k < lo || k > hi) return false;
-    if (FAST || K <= kExactChunk || (k > lo + 1 && k < hi - 1)) return true;
+    if (K <= kExactChunk || (k > lo + 1 && k < hi - 1)) return true;
     float4 m4 = __ldg(reinterpret_cast<const float4*>(a.rec + leaf));
     return slab_hit_exact(a, leaf, f3(m4.x, m4.y, m4.z), r);
 }
 
 // Sample buffers of slab k: sum of density and density-weighted colour of the lane's hits.
 template <bool FAST, int CAP>
-__device__ __forceinline__ int slab_buffers(const WarpSmem<CAP>& sm, int k, int K, bool has, const RayState& r,
+__device__ __forceinline__ int slab_buffers(const WarpSmem<FAST, CAP>& sm, int k, int K, bool has, const RayState& r,
                                             const RenderArgs& a, long long rgb_base, const float* roff,
-                                            float* sig, float3* C, int lane) {
+                                            float* sig, float3* C, int lane, WarpStats& ws) {
     int nh = 0;
 #pragma unroll 1
     for (int w = 0; w < CAP / 32; ++w) {
@@ -385,9 +406,10 @@ __device__ __forceinline__ int slab_buffers(const WarpSmem<CAP>& sm, int k, int 
         while (mw) {
             const int e = 32 * w + __ffs(mw) - 1;
             mw &= mw - 1u;
+            ++ws.entry_slabs;
             if (!has) continue;
             const int leaf = sm.ids[e];
-            if (!lane_has_entry<FAST>(a, sm.lrng[e][lane], k, K, leaf, r)) continue;
+            if (!lane_has_entry<FAST, CAP>(sm, a, e, k, K, leaf, r, lane)) continue;
             LeafRec rec = load_rec(a.rec, leaf);
             float4 col4 = __ldg(a.rgb + rgb_base + leaf);
             float3 mu = f3(rec.a.x, rec.a.y, rec.a.z);
@@ -510,9 +532,10 @@ __device__ __forceinline__ float transpose_reduce16(float* v, int lane) {
 // Adjoint of slab k for all list entries: per-lane gradient of each hit Gaussian, warp reduction,
 // one atomic per value.  Value order: ddens, dpos.xyz, dscale.xyz, dquat.xyzw, drgb.xyz.
 template <bool FAST, int CAP>
-__device__ __forceinline__ void slab_adjoint(const WarpSmem<CAP>& sm, int k, int K, bool has, const RayState& r,
+__device__ __forceinline__ void slab_adjoint(const WarpSmem<FAST, CAP>& sm, int k, int K, bool has, const RayState& r,
                                              const RenderArgs& a, long long rgb_base, const float* roff,
-                                             const float* E, const float* F, const float* G, int lane) {
+                                             const float* E, const float* F, const float* G, int lane,
+                                             WarpStats& ws) {
     const int vid = ((lane >> 4) & 1) * 8 + ((lane >> 3) & 1) * 4 + ((lane >> 2) & 1) * 2 + ((lane >> 1) & 1);
 #pragma unroll 1
     for (int w = 0; w < CAP / 32; ++w) {
@@ -521,7 +544,8 @@ __device__ __forceinline__ void slab_adjoint(const WarpSmem<CAP>& sm, int k, int
         const int e = 32 * w + __ffs(mw) - 1;
         mw &= mw - 1u;
         const int leaf = sm.ids[e];
-        bool act = has && lane_has_entry<FAST>(a, sm.lrng[e][lane], k, K, leaf, r);
+        ++ws.entry_slabs;
+        bool act = has && lane_has_entry<FAST, CAP>(sm, a, e, k, K, leaf, r, lane);
         unsigned am = __ballot_sync(kFull, act);
         if (am == 0u) continue;
         float v[16];
@@ -653,16 +677,18 @@ __device__ __forceinline__ void slab_adjoint_scalars(const RayState& r, const fl
 
 template <bool BWD, bool FAST, int CAP>
 __global__ void __launch_bounds__(kWarpsPerBlock * 32) k_render(RenderArgs a) {
-    __shared__ WarpSmem<CAP> smem[kWarpsPerBlock];
+    __shared__ WarpSmem<FAST, CAP> smem[kWarpsPerBlock];
     const int lane = threadIdx.x & 31;
-    WarpSmem<CAP>& sm = smem[threadIdx.x >> 5];
+    WarpSmem<FAST, CAP>& sm = smem[threadIdx.x >> 5];
     const ViewTable* vt = a.views;
     const float bg = a.white_bg ? 1.f : 0.f;
     float scene[6];
 #pragma unroll
     for (int z = 0; z < 6; ++z) scene[z] = ord2f(a.scene_ord[z]);
     unsigned long long hits_acc = 0, slabs_acc = 0;
-    const int kmax = min((a.rnd_sample == 1) ? min(a.chunk_slabs, kExactChunk) : a.chunk_slabs, kMaskChunk);
+    WarpStats ws;
+    const int kmax =
+        min((a.rnd_sample == 1) ? min(a.chunk_slabs, kExactChunk) : a.chunk_slabs, WarpSmem<FAST, CAP>::KM);
 
     while (true) {
         int tile = 0;
@@ -760,7 +786,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32) k_render(RenderArgs a) {
                 if (!(r.tb < r.texit) || r.tb + kSlab == r.tb) { r.alive = false; on = false; nv = 0; }
             }
             bool ovf;
-            int count = traverse<FAST, CAP>(sm, a, r, on, seg_hi, K, nv, -1, ovf, lane);
+            int count = traverse<FAST, CAP>(sm, a, r, on, seg_hi, K, nv, -1, ovf, lane, ws);
             const unsigned long long* occ = sm.occ;
             if (ovf && K > 1) {
                 K = max(1, K >> 1);
@@ -783,13 +809,14 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32) k_render(RenderArgs a) {
                         k = k2 - 1;
                         continue;
                     }
+                    ++ws.slab_steps;
                     float roff[kBuf];
                     unsigned seed_next = slab_offsets(a.rnd_sample, r.seed, roff);
                     float sig[kBuf];
                     float3 Cb[kBuf];
 #pragma unroll
                     for (int i = 0; i < kBuf; ++i) { sig[i] = 0.f; Cb[i] = f3(0.f, 0.f, 0.f); }
-                    int nh = slab_buffers<FAST, CAP>(sm, k, K, has, r, a, rgb_base, roff, sig, Cb, lane);
+                    int nh = slab_buffers<FAST, CAP>(sm, k, K, has, r, a, rgb_base, roff, sig, Cb, lane, ws);
                     if (has) {
                         ++slabs_acc;
                         hits_acc += nh;
@@ -805,7 +832,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32) k_render(RenderArgs a) {
                         float3 Ra;
                         slab_adjoint_scalars<FAST>(r, sig, Cb, E, F, G, Ta, Ra);
                         bool act = has && nh > 0;
-                        slab_adjoint<FAST, CAP>(sm, k, K, act, r, a, rgb_base, roff, E, F, G, lane);
+                        slab_adjoint<FAST, CAP>(sm, k, K, act, r, a, rgb_base, roff, E, F, G, lane, ws);
                         if (act) {
                             r.T = Ta;
                             r.C = Ra;
@@ -814,7 +841,11 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32) k_render(RenderArgs a) {
                     }
                     if (has) r.tb = r.tb + kSlab;
                 }
-                if (count < CAP / 4 && K < kmax) K = min(kmax, K << 1);
+                // next chunk length: aim at half a list, grow at most 2x per chunk
+                {
+                    int target = count > 0 ? (K * (CAP / 2)) / count : kmax;
+                    K = max(1, min(kmax, min(2 * K, target)));
+                }
             } else {
                 // K == 1 and more hits than the list holds: consume the slab in several passes
                 bool has = on && nv > 0 && r.T > kTeps;
@@ -824,14 +855,14 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32) k_render(RenderArgs a) {
                 float3 Cb[kBuf];
 #pragma unroll
                 for (int i = 0; i < kBuf; ++i) { sig[i] = 0.f; Cb[i] = f3(0.f, 0.f, 0.f); }
-                int nh = slab_buffers<FAST, CAP>(sm, 0, 1, has, r, a, rgb_base, roff, sig, Cb, lane);
+                int nh = slab_buffers<FAST, CAP>(sm, 0, 1, has, r, a, rgb_base, roff, sig, Cb, lane, ws);
                 bool more = ovf;
                 while (more) {
                     int cursor = sm.ids[count - 1];
                     __syncwarp();
                     if (lane == 0) atomicAdd(&a.st->list_passes, 1ull);
-                    count = traverse<FAST, CAP>(sm, a, r, on, seg_hi, 1, nv, cursor, more, lane);
-                    nh += slab_buffers<FAST, CAP>(sm, 0, 1, has, r, a, rgb_base, roff, sig, Cb, lane);
+                    count = traverse<FAST, CAP>(sm, a, r, on, seg_hi, 1, nv, cursor, more, lane, ws);
+                    nh += slab_buffers<FAST, CAP>(sm, 0, 1, has, r, a, rgb_base, roff, sig, Cb, lane, ws);
                 }
                 if (has) {
                     ++slabs_acc;
@@ -851,8 +882,8 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32) k_render(RenderArgs a) {
                     int cursor = -1;
                     bool more2 = true;
                     while (more2) {
-                        count = traverse<FAST, CAP>(sm, a, r, on, seg_hi, 1, nv, cursor, more2, lane);
-                        slab_adjoint<FAST, CAP>(sm, 0, 1, act, r, a, rgb_base, roff, E, F, G, lane);
+                        count = traverse<FAST, CAP>(sm, a, r, on, seg_hi, 1, nv, cursor, more2, lane, ws);
+                        slab_adjoint<FAST, CAP>(sm, 0, 1, act, r, a, rgb_base, roff, E, F, G, lane, ws);
                         if (more2) cursor = sm.ids[count - 1];
                         __syncwarp();
                     }
@@ -881,22 +912,35 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32) k_render(RenderArgs a) {
     if (lane == 0) {
         atomicAdd(&a.st->hit_pairs, hits_acc);
         atomicAdd(&a.st->slabs, slabs_acc);
+        atomicAdd(&a.st->traversals, ws.traversals);
+        atomicAdd(&a.st->node_visits, ws.node_visits);
+        atomicAdd(&a.st->leaf_tests, ws.leaf_tests);
+        atomicAdd(&a.st->list_entries, ws.entries);
+        atomicAdd(&a.st->slab_steps, ws.slab_steps);
+        atomicAdd(&a.st->entry_slabs, ws.entry_slabs);
     }
 }
 
 int render_block_threads() { return kWarpsPerBlock * 32; }
 
+// List capacity per arithmetic: the tuning value (64 or 128) for parity, 4x for fast.
 size_t render_smem_bytes(bool, int cap) {
-    if (cap <= 64) return sizeof(WarpSmem<64>) * kWarpsPerBlock;
-    return sizeof(WarpSmem<128>) * kWarpsPerBlock;
+    if (cap <= 64) return sizeof(WarpSmem<false, 64>) * kWarpsPerBlock;
+    return sizeof(WarpSmem<false, 128>) * kWarpsPerBlock;
 }
-static_assert(sizeof(WarpSmem<128>) * kWarpsPerBlock <= 48 * 1024, "static shared memory limit");
+static_assert(sizeof(WarpSmem<false, 128>) * kWarpsPerBlock <= 48 * 1024, "static shared memory limit");
+static_assert(sizeof(WarpSmem<true, 512>) * kWarpsPerBlock <= 48 * 1024, "static shared memory limit");
 
 template <bool BWD, bool FAST>
 static cudaError_t launch_cap(int cap, int grid, const RenderArgs& a, cudaStream_t s) {
     const int threads = kWarpsPerBlock * 32;
-    if (cap <= 64) k_render<BWD, FAST, 64><<<grid, threads, 0, s>>>(a);
-    else k_render<BWD, FAST, 128><<<grid, threads, 0, s>>>(a);
+    if constexpr (FAST) {
+        if (cap <= 64) k_render<BWD, FAST, 256><<<grid, threads, 0, s>>>(a);
+        else k_render<BWD, FAST, 512><<<grid, threads, 0, s>>>(a);
+    } else {
+        if (cap <= 64) k_render<BWD, FAST, 64><<<grid, threads, 0, s>>>(a);
+        else k_render<BWD, FAST, 128><<<grid, threads, 0, s>>>(a);
+    }
     return cudaGetLastError();
 }
 
@@ -904,8 +948,13 @@ template <bool BWD, bool FAST>
 static int occ_cap(int cap) {
     int nb = 0;
     const int threads = kWarpsPerBlock * 32;
-    if (cap <= 64) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_render<BWD, FAST, 64>, threads, 0);
-    else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_render<BWD, FAST, 128>, threads, 0);
+    if constexpr (FAST) {
+        if (cap <= 64) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_render<BWD, FAST, 256>, threads, 0);
+        else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_render<BWD, FAST, 512>, threads, 0);
+    } else {
+        if (cap <= 64) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_render<BWD, FAST, 64>, threads, 0);
+        else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_render<BWD, FAST, 128>, threads, 0);
+    }
     return nb;
 }
 
