@@ -202,6 +202,17 @@ RG_API int rg_render_backward(rg_engine* e, const rg_gaussians* g, const rg_came
  * device).  Hits of a slab are accumulated in increasing leaf order; the reference's order is
  * its (unspecified) traversal order.  No reference counterpart (introspection of the BVH). */
 RG_API int rg_leaf_order(rg_engine* e, int32_t* leaf_gid_out, void* stream);
+/* Allocation-free forward render for callers that cannot call cudaMalloc (allocation-free graph
+ * capture, fixed device-memory budgets, plugins that must not touch the process allocator).  No
+ * counterpart in the reference.  Same pre-pass, LBVH build, colour pass and forward launch as
+ * rg_render_forward (default tuning), without an engine: all scratch lives in one static device
+ * array of about 9 MB that every GPU loading this library keeps until exit.  At most 16384
+ * Gaussians and 4 views per call (RG_ERR_CAPACITY beyond).  Calls share that array, so calls that
+ * overlap on the GPU race; the first call on a device resolves the array's address and should
+ * come before any stream capture.  cams, ray_colors and final_T are device pointers as in
+ * rg_launch_forward; final_T may be NULL. */
+RG_API int rg_render_forward_noalloc(const rg_gaussians* g, const rg_camera* cams, int32_t n_cams,
+                                     const rg_settings* s, float* ray_colors, float* final_T, void* stream);
 /* Read (and optionally reset) the device counters; synchronises the engine's last stream. */
 RG_API int rg_get_status(rg_engine* e, rg_status* out, int32_t reset, void* stream);
 /* Number of kernels launched by this engine since creation (for launch accounting). */

@@ -94,6 +94,8 @@ SIGNATURES = {
                                           ctypes.POINTER(rg_settings), _P, _P, ctypes.POINTER(rg_gradients), _P]),
     "rg_get_status": (ctypes.c_int, [_P, ctypes.POINTER(rg_status), ctypes.c_int32, _P]),
     "rg_leaf_order": (ctypes.c_int, [_P, _P, _P]),
+    "rg_render_forward_noalloc": (ctypes.c_int, [ctypes.POINTER(rg_gaussians), _P, ctypes.c_int32,
+                                                 ctypes.POINTER(rg_settings), _P, _P, _P]),
 }
 
 _LOCK = threading.Lock()
