@@ -189,7 +189,7 @@ extern "C" RG_API int rg_render_forward_noalloc(const rg_gaussians* g, const rg_
     a.rnd_sample = s->rnd_sample;
     a.max_prim_slice = s->max_prim_slice > 0 ? s->max_prim_slice : 1024;
     a.iteration = s->iteration;
-    a.chunk_slabs = 128;  // the engine's default tuning
+    a.chunk_slabs = 64;  // the engine's default tuning
     a.work_counter = work;
     a.st = status;
     a.ray_colors = ray_colors;

@@ -53,12 +53,14 @@ constexpr int kExactChunk = 8;             // chunks up to this length use exact
 // regions.
 template <bool FAST, int CAP>
 struct WarpSmem {
-    static constexpr int KM = FAST ? 64 : 128;      // longest chunk (slab entry masks per slab)
+    static constexpr int MB = FAST ? 4 : 2;         // slabs per entry-mask block
+    static constexpr int NB = 64;                   // entry-mask blocks
+    static constexpr int KM = FAST ? 255 : 128;     // longest chunk (MB * NB, slab ranges are bytes)
     int ids[CAP];
     unsigned urng[CAP];                              // union of the lanes' slab ranges: lo | hi << 16
     unsigned lmask[FAST ? CAP : 1];                  // fast: lanes whose interval overlaps the chunk
     unsigned short lrng[FAST ? 1 : CAP][32];         // parity: per lane lo | hi << 8 (lo > hi: no hit)
-    unsigned smask[KM][CAP / 32];                    // entries whose union range holds slab k
+    unsigned smask[NB][CAP / 32];                    // entries whose union range meets block k / MB
     unsigned long long occ[4];                       // slabs holding any entry (union occupancy)
     int stack[kStack];
 };
@@ -315,8 +317,11 @@ __device__ int traverse(WarpSmem<FAST, CAP>& sm, const RenderArgs& a, const RayS
         for (int w = 0; w < 4; ++w) sm.occ[w] = occ[w];
     }
     ws.entries += count;
-    // per-slab entry masks: lane l fills slabs l, l+32, ...
-    for (int k = lane; k < K; k += 32) {
+    // entry masks per block of MB slabs: lane l fills blocks l, l+32
+    constexpr int MB = WarpSmem<FAST, CAP>::MB;
+    const int nblk = (K + MB - 1) / MB;
+    for (int bk = lane; bk < nblk; bk += 32) {
+        const int k0 = bk * MB, k1 = k0 + MB - 1;
 #pragma unroll
         for (int w = 0; w < CAP / 32; ++w) {
             unsigned mw = 0u;
@@ -324,9 +329,9 @@ __device__ int traverse(WarpSmem<FAST, CAP>& sm, const RenderArgs& a, const RayS
 #pragma unroll 1
             for (int e = e0; e < e1; ++e) {
                 unsigned u = sm.urng[e];
-                if (k >= (int)(u & 0xffff) && k <= (int)(u >> 16)) mw |= 1u << (e - e0);
+                if (k1 >= (int)(u & 0xffff) && k0 <= (int)(u >> 16)) mw |= 1u << (e - e0);
             }
-            sm.smask[k][w] = mw;
+            sm.smask[bk][w] = mw;
         }
     }
     __syncwarp();
@@ -402,10 +407,11 @@ __device__ __forceinline__ int slab_buffers(const WarpSmem<FAST, CAP>& sm, int k
     int nh = 0;
 #pragma unroll 1
     for (int w = 0; w < CAP / 32; ++w) {
-        unsigned mw = sm.smask[k][w];
+        unsigned mw = sm.smask[k / WarpSmem<FAST, CAP>::MB][w];
         while (mw) {
             const int e = 32 * w + __ffs(mw) - 1;
             mw &= mw - 1u;
+            if (!in_urange(sm.urng[e], k)) continue;
             ++ws.entry_slabs;
             if (!has) continue;
             const int leaf = sm.ids[e];
@@ -539,10 +545,11 @@ __device__ __forceinline__ void slab_adjoint(const WarpSmem<FAST, CAP>& sm, int 
     const int vid = ((lane >> 4) & 1) * 8 + ((lane >> 3) & 1) * 4 + ((lane >> 2) & 1) * 2 + ((lane >> 1) & 1);
 #pragma unroll 1
     for (int w = 0; w < CAP / 32; ++w) {
-      unsigned mw = sm.smask[k][w];
+      unsigned mw = sm.smask[k / WarpSmem<FAST, CAP>::MB][w];
       while (mw) {
         const int e = 32 * w + __ffs(mw) - 1;
         mw &= mw - 1u;
+        if (!in_urange(sm.urng[e], k)) continue;
         const int leaf = sm.ids[e];
         ++ws.entry_slabs;
         bool act = has && lane_has_entry<FAST, CAP>(sm, a, e, k, K, leaf, r, lane);
