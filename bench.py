@@ -76,6 +76,17 @@ def _clock_summary(proc):
             "samples": len(sm)}
 
 
+def max_over_ranks(value: float, device) -> float:
+    """Max of a per-rank scalar over the process group (the step time of the slowest replica)."""
+    import torch
+    import torch.distributed as dist
+    if not (dist.is_available() and dist.is_initialized()) or dist.get_world_size() == 1:
+        return float(value)
+    t = torch.tensor([float(value)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
 def _peaks():
     try:
         with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
@@ -102,6 +113,8 @@ def main():
     ap.add_argument("--no-plain", action="store_true", help="skip the plain single-view comparison")
     ap.add_argument("--no-cpu", action="store_true", help="skip the host-core baseline")
     ap.add_argument("--cpu-rays", type=int, default=256, help="rays per view in the host-core sample")
+    ap.add_argument("--no-tune", action="store_true", help="skip the autotuner (engine defaults)")
+    ap.add_argument("--no-graph", action="store_true", help="skip the CUDA-graph replay measurement")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
@@ -170,6 +183,12 @@ def our_arm(args, rank, world, local):
             import torch.distributed as dist
             dist.barrier()
 
+    # ---- autotune the render kernels on this scene and these views (a few launches) ----
+    tuning = eng.get_tuning()
+    if not args.no_tune:
+        from ray_gauss_b200.autotune import autotune
+        tuning = autotune(Pb, views, target, repeats=1, chunks=(32, 64, 128), capacities=(128,), ctas=(0,))
+
     # ---- headline: batched BF16-storage form (device-resident inputs) ----
     for _ in range(args.warmup):
         zero(leaves)
@@ -195,12 +214,7 @@ def our_arm(args, rank, world, local):
     launches = eng.kernel_launches() - launches0
     timers, eng.timers = eng.timers, None
     st = eng.status()
-    ms_max = ms
-    if world > 1:
-        import torch.distributed as dist
-        t = torch.tensor([ms], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms_max = float(t.item())
+    ms_max = max_over_ranks(ms, dev)
     value = world * R / (ms_max * 1e-3) / 1e6
 
     # dominant kernel: the backward launch (events on the launching stream)
@@ -225,6 +239,27 @@ def our_arm(args, rank, world, local):
     p_store = bytes_per_gaussian(nsg, ncoef, True)
     g_bytes = bytes_per_gaussian(nsg, ncoef, False)
     b_step = 2 * n * p_store + n * g_bytes + 36 * R
+
+    # ---- the same step captured as one CUDA graph (refit + forward + loss + backward) ----
+    graph = None
+    if not args.no_graph:
+        from ray_gauss_b200.graph import GraphedStep
+        gleaves = {k: v.detach().clone() for k, v in Pb.items()}
+        gstep = GraphedStep(gleaves, views, target)
+        gstep.replay()
+        torch.cuda.synchronize()
+        g0 = torch.cuda.Event(enable_timing=True)
+        g1 = torch.cuda.Event(enable_timing=True)
+        g0.record()
+        for _ in range(args.steps):
+            gstep.replay()
+        g1.record()
+        torch.cuda.synchronize()
+        g_ms = g0.elapsed_time(g1) / args.steps
+        graph = {"value": round(R / (g_ms * 1e-3) / 1e6, 3), "unit": "Mrays/s", "ms_per_step": round(g_ms, 3),
+                 "form": "GraphedStep.replay(): LBVH refit + colour + forward + MSE + backward in one CUDA graph"}
+        views.update = False
+        del gstep, gleaves
 
     # ---- e2e through the public API: host parameters and targets in, loss out ----
     e2e = None
@@ -325,6 +360,8 @@ def our_arm(args, rank, world, local):
         "stage_ms": {"prepare(bbox+bvh+colour)": round(prep_ms, 3), "forward": round(fwd_ms, 3),
                      "backward": round(bwd_ms, 3), "backward_sh": round(shb_ms, 3)},
         "counters_per_step": {k: v // max(1, args.steps) for k, v in st.items()},
+        "tuning": {k: v for k, v in tuning.items() if k != "ms"},
+        "graph_replay": graph,
         "plain_fp32_single_view": plain,
         "batched_over_plain": round(value / world / plain["value"], 3) if plain else None,
         "accuracy": accuracy,
@@ -383,8 +420,10 @@ def _host_side(args, p_host, cams, white, views, leaves, Pb, eng):
 
 
 def reference_arm(args, rank, world):
-    """The reference's CPU implementation of the path on the host cores (oracle/_ref when built here,
-    else the C restatement), bounded sample, same metric and unit."""
+    """The reference's own CPU implementation of the path on the host cores: its training device
+    programs (cuda_train/forward and backward gaussians_aabb.cu, utils/sh_utils.cu) compiled for the
+    CPU under oracle/_ref when that build is present, otherwise the C restatement; bounded sample of
+    rays per step, same metric and unit."""
     if rank != 0:
         return 0
     from oracle import oracle as O
@@ -392,32 +431,49 @@ def reference_arm(args, rank, world):
     p, cams, white = S.workload(WORKLOAD, seed=0, device="cpu", n=args.n)
     cams = cams[: args.views]
     Pn = {k: v.numpy().astype(np.float32) for k, v in p.items()}
-    cam = cams[0]
-    W, H = cam.image_width, cam.image_height
-    cv = O.camera_vector(cam)
-    rgb = O.forward_sh(cv[:3], Pn["positions"], Pn["color_features"], Pn["sph_gauss_features"],
-                       Pn["bandwidth_sharpness"], Pn["lobe_axis"])
-    aabb, box = O.bbox(Pn["positions"], Pn["scales"], Pn["quaternions"], Pn["densities"], "f32")
+    use_ref = O.ref_available()
     rng = np.random.default_rng(3)
+    rays = max(8, args.cpu_rays // 8) if use_ref else max(16, args.cpu_rays // 4)
+    prepared = []
+    for cam in cams[:2]:
+        cv = O.camera_vector(cam)
+        sh = (Pn["color_features"], Pn["sph_gauss_features"], Pn["bandwidth_sharpness"], Pn["lobe_axis"])
+        rgb = O.ref_forward_sh(cv[:3], Pn["positions"], *sh) if use_ref else O.forward_sh(cv[:3], Pn["positions"], *sh)
+        aabb, box = O.bbox(Pn["positions"], Pn["scales"], Pn["quaternions"], Pn["densities"], "f32")
+        prepared.append((cam, cv, rgb, aabb, box))
     times = []
-    rays = max(16, args.cpu_rays // 4)
     for s in range(args.warmup + args.steps):
+        cam, cv, rgb, aabb, box = prepared[s % len(prepared)]
+        W, H = cam.image_width, cam.image_height
         ids = rng.integers(0, W * H, rays).astype(np.int32)
         t = time.perf_counter()
-        img, _, _ = O.render_forward(Pn["positions"], Pn["scales"], Pn["quaternions"], Pn["densities"], rgb, cv, W, H,
-                                     white, ray_ids=ids, aabb=aabb, scene_box=box, prec="f32")
-        O.render_backward(Pn["positions"], Pn["scales"], Pn["quaternions"], Pn["densities"], rgb, cv, W, H, img,
-                          np.full(img.shape, 1e-3, np.float32), ray_ids=ids, aabb=aabb, scene_box=box, prec="f32")
+        if use_ref:
+            img, _ = O.ref_render_forward(Pn["positions"], Pn["scales"], Pn["quaternions"], Pn["densities"], rgb, cv,
+                                          W, H, white, aabb=aabb, scene_box=box, ray_ids=ids)
+            dL = np.zeros_like(img)
+            dL[ids] = 1e-3
+            O.ref_render_backward(Pn["positions"], Pn["scales"], Pn["quaternions"], Pn["densities"], rgb, cv, W, H,
+                                  img, dL, aabb=aabb, scene_box=box, ray_ids=ids)
+        else:
+            img, _, _ = O.render_forward(Pn["positions"], Pn["scales"], Pn["quaternions"], Pn["densities"], rgb, cv,
+                                         W, H, white, ray_ids=ids, aabb=aabb, scene_box=box, prec="f32")
+            O.render_backward(Pn["positions"], Pn["scales"], Pn["quaternions"], Pn["densities"], rgb, cv, W, H, img,
+                              np.full(img.shape, 1e-3, np.float32), ray_ids=ids, aabb=aabb, scene_box=box,
+                              prec="f32")
         if s >= args.warmup:
             times.append(time.perf_counter() - t)
     ms = statistics.mean(times) * 1e3
     value = rays / (ms * 1e-3) / 1e6
+    kind = "reference" if use_ref else "port"
+    what = ("the reference's training device programs compiled for the CPU (oracle/_ref; OptiX traversal "
+            "emulated by a per-ray candidate list)" if use_ref else "the C restatement (oracle/liboracle.so)")
     line = {"impl": "reference", "metric": METRIC, "value": round(value, 6), "unit": "Mrays/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms, 3), "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": f"{WORKLOAD} view 0, {rays} random rays per step"},
-            "cpu_baseline": {"value": round(value, 6), "unit": "Mrays/s", "cores": O.num_threads(), "kind": "port",
-                             "sample": f"{rays} random rays of view 0 per step, FP32 forward+backward"},
+            "config": {"workload": f"{WORKLOAD}: {args.n} Gaussians, views 0-1, {rays} random rays per step, "
+                                   "FP32 forward+backward on host cores"},
+            "cpu_baseline": {"value": round(value, 6), "unit": "Mrays/s", "cores": O.num_threads(), "kind": kind,
+                             "sample": f"{rays} random rays of views 0/1 per step, forward+backward, {what}"},
             "e2e": {"value": round(value, 6), "unit": "Mrays/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line))
     return 0

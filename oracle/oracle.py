@@ -186,7 +186,9 @@ def render_backward(pos, scl, quat, dens, rgb, cam_vec, width, height, ray_color
 # ---- the reference's own device programs, compiled for the CPU (oracle/_ref) ------------------
 
 def ref_render_forward(pos, scl, quat, dens, rgb, cam_vec, width, height, white_bg=True, max_prim_slice=1024,
-                       jitter=0, rnd_sample=0, iteration=0, aabb=None, scene_box=None):
+                       jitter=0, rnd_sample=0, iteration=0, aabb=None, scene_box=None, ray_ids=None):
+    """The reference forward program; with ``ray_ids`` only those rays are launched and the
+    full (W*H, 3) image holds zeros elsewhere."""
     f = np.float32
     pos, scl, quat, dens, rgb = (_c(a, f) for a in (pos, scl, quat, dens, rgb))
     if aabb is None or scene_box is None:
@@ -194,17 +196,18 @@ def ref_render_forward(pos, scl, quat, dens, rgb, cam_vec, width, height, white_
     aabb, scene_box, cam = _c(aabb, f), _c(scene_box, f), _c(cam_vec, f)
     out = np.zeros((width * height, 3), f)
     ovf = np.zeros(1, np.int32)
+    ids = None if ray_ids is None else _c(ray_ids, np.int32)
     rc = _ref("fwd").ref_forward(
         ctypes.c_int(pos.shape[0]), _p(pos), _p(scl), _p(quat), _p(dens), _p(rgb), _p(aabb), _p(scene_box),
         _p(cam), ctypes.c_int(width), ctypes.c_int(height), ctypes.c_int(int(bool(white_bg))),
         ctypes.c_int(max_prim_slice), ctypes.c_int(jitter), ctypes.c_int(rnd_sample), ctypes.c_uint(iteration),
-        _p(out), _p(ovf))
+        _p(ids), ctypes.c_int(0 if ids is None else ids.shape[0]), _p(out), _p(ovf))
     assert rc == 0
     return out, int(ovf[0])
 
 
 def ref_render_backward(pos, scl, quat, dens, rgb, cam_vec, width, height, ray_colors, dL, max_prim_slice=1024,
-                        jitter=0, rnd_sample=0, iteration=0, aabb=None, scene_box=None):
+                        jitter=0, rnd_sample=0, iteration=0, aabb=None, scene_box=None, ray_ids=None):
     f = np.float32
     pos, scl, quat, dens, rgb = (_c(a, f) for a in (pos, scl, quat, dens, rgb))
     if aabb is None or scene_box is None:
@@ -214,10 +217,12 @@ def ref_render_backward(pos, scl, quat, dens, rgb, cam_vec, width, height, ray_c
     n = pos.shape[0]
     g = {k: np.zeros(s, f) for k, s in
          (("d_rgb", (n, 3)), ("d_dens", (n,)), ("d_pos", (n, 3)), ("d_scl", (n, 3)), ("d_quat", (n, 4)))}
+    ids = None if ray_ids is None else _c(ray_ids, np.int32)
     rc = _ref("bwd").ref_backward(
         ctypes.c_int(n), _p(pos), _p(scl), _p(quat), _p(dens), _p(rgb), _p(aabb), _p(scene_box), _p(cam),
         ctypes.c_int(width), ctypes.c_int(height), ctypes.c_int(max_prim_slice), ctypes.c_int(jitter),
-        ctypes.c_int(rnd_sample), ctypes.c_uint(iteration), _p(ray_colors), _p(dL), _p(g["d_dens"]),
+        ctypes.c_int(rnd_sample), ctypes.c_uint(iteration), _p(ids), ctypes.c_int(0 if ids is None else ids.shape[0]),
+        _p(ray_colors), _p(dL), _p(g["d_dens"]),
         _p(g["d_rgb"]), _p(g["d_pos"]), _p(g["d_scl"]), _p(g["d_quat"]))
     assert rc == 0
     return g

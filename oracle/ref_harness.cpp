@@ -42,10 +42,12 @@ static void set_common(int n, const float* pos, const float* scl, const float* q
 
 static sphere::SphereHitGroupData g_sbt;
 
-static void run_rays(int n_rays, int W, int H) {
+/* Launch the ray-generation program for rays ids[0..n_ids) (all W*H rays when ids is null). */
+static void run_rays(int W, int H, const int* ids, int n_ids) {
+    const int n_rays = ids ? n_ids : W * H;
 #pragma omp parallel for schedule(dynamic, 8)
     for (int r = 0; r < n_rays; ++r) {
-        rg_emul.launch_idx = make_uint3((unsigned)r, 0u, 0u);
+        rg_emul.launch_idx = make_uint3((unsigned)(ids ? ids[r] : r), 0u, 0u);
         rg_emul.launch_dim = make_uint3((unsigned)(W * H), 1u, 1u);
         rg_emul.have_cands = false;
         __raygen__rg();
@@ -57,7 +59,9 @@ static void run_rays(int n_rays, int W, int H) {
 extern "C" int ref_forward(int n, const float* pos, const float* scl, const float* quat, const float* dens,
                            const float* rgb, const float* aabb, const float* scene_box, const float* cam,
                            int W, int H, int white_bg, int max_prim_slice, int jitter, int rnd_sample,
-                           unsigned iteration, float* out_colors, int* overflow) {
+                           unsigned iteration, const int* ids, int n_ids, float* out_colors, int* overflow) {
+    /* W*H*max_prim_slice slots as the reference allocates them (scripts/train.py:38-39); only the
+     * pages of launched rays are touched */
     int* hit_buf = (int*)std::calloc((size_t)W * H * (size_t)max_prim_slice, sizeof(int));
     if (!hit_buf) return -1;
     set_common(n, pos, scl, quat, dens, rgb, scene_box, cam, W, H, max_prim_slice, jitter, rnd_sample,
@@ -69,7 +73,7 @@ extern "C" int ref_forward(int n, const float* pos, const float* scl, const floa
     params.white_background = (unsigned)white_bg;
     g_sbt.positions = (float3*)pos; g_sbt.scales = (float3*)scl; g_sbt.quaternions = (float4*)quat;
     rg_emul_scene.aabb = aabb; rg_emul_scene.n = n; rg_emul_scene.sbt_data = &g_sbt;
-    run_rays(W * H, W, H);
+    run_rays(W, H, ids, n_ids);
     std::free(hit_buf);
     return 0;
 }
@@ -77,8 +81,8 @@ extern "C" int ref_forward(int n, const float* pos, const float* scl, const floa
 extern "C" int ref_backward(int n, const float* pos, const float* scl, const float* quat, const float* dens,
                             const float* rgb, const float* aabb, const float* scene_box, const float* cam,
                             int W, int H, int max_prim_slice, int jitter, int rnd_sample, unsigned iteration,
-                            const float* ray_colors, const float* dL, float* d_dens, float* d_rgb,
-                            float* d_pos, float* d_scl, float* d_quat) {
+                            const int* ids, int n_ids, const float* ray_colors, const float* dL, float* d_dens,
+                            float* d_rgb, float* d_pos, float* d_scl, float* d_quat) {
     int* hit_buf = (int*)std::calloc((size_t)W * H * (size_t)max_prim_slice, sizeof(int));
     if (!hit_buf) return -1;
     set_common(n, pos, scl, quat, dens, rgb, scene_box, cam, W, H, max_prim_slice, jitter, rnd_sample,
@@ -93,7 +97,7 @@ extern "C" int ref_backward(int n, const float* pos, const float* scl, const flo
     params.handle = 0;
     g_sbt.positions = (float3*)pos; g_sbt.scales = (float3*)scl; g_sbt.quaternions = (float4*)quat;
     rg_emul_scene.aabb = aabb; rg_emul_scene.n = n; rg_emul_scene.sbt_data = &g_sbt;
-    run_rays(W * H, W, H);
+    run_rays(W, H, ids, n_ids);
     std::free(hit_buf);
     return 0;
 }
