@@ -202,6 +202,9 @@ __device__ __forceinline__ void slab_range(const RayState& r, int K, int nv, flo
     }
 }
 
+// 32-entry mask words holding `count` list entries.
+__device__ __forceinline__ int nwords(int count) { return (count + 31) >> 5; }
+
 // Union occupancy of the chunk's slabs (256 bits): bit k set when some lane has a hit in slab k.
 __device__ __forceinline__ void occ_set(unsigned long long* occ, int lo, int hi) {
 #pragma unroll
@@ -320,10 +323,11 @@ __device__ int traverse(WarpSmem<FAST, CAP>& sm, const RenderArgs& a, const RayS
     // entry masks per block of MB slabs: lane l fills blocks l, l+32
     constexpr int MB = WarpSmem<FAST, CAP>::MB;
     const int nblk = (K + MB - 1) / MB;
+    const int nw = nwords(count);
     for (int bk = lane; bk < nblk; bk += 32) {
         const int k0 = bk * MB, k1 = k0 + MB - 1;
-#pragma unroll
-        for (int w = 0; w < CAP / 32; ++w) {
+#pragma unroll 1
+        for (int w = 0; w < nw; ++w) {
             unsigned mw = 0u;
             const int e0 = 32 * w, e1 = min(count, e0 + 32);
 #pragma unroll 1
@@ -403,10 +407,10 @@ __device__ __forceinline__ bool lane_has_entry(const WarpSmem<FAST, CAP>& sm, co
 template <bool FAST, int CAP>
 __device__ __forceinline__ int slab_buffers(const WarpSmem<FAST, CAP>& sm, int k, int K, bool has, const RayState& r,
                                             const RenderArgs& a, long long rgb_base, const float* roff,
-                                            float* sig, float3* C, int lane, WarpStats& ws) {
+                                            float* sig, float3* C, int nw, int lane, WarpStats& ws) {
     int nh = 0;
 #pragma unroll 1
-    for (int w = 0; w < CAP / 32; ++w) {
+    for (int w = 0; w < nw; ++w) {
         unsigned mw = sm.smask[k / WarpSmem<FAST, CAP>::MB][w];
         while (mw) {
             const int e = 32 * w + __ffs(mw) - 1;
@@ -465,15 +469,25 @@ __device__ __forceinline__ float exp_neg(float x) {
     return FAST ? ex2_approx(-x * 1.4426950408889634f) : (float)exp(-(double)x);
 }
 
+__device__ __forceinline__ bool any_density(const float* sig) {
+    bool any = false;
+#pragma unroll
+    for (int i = 0; i < kBuf; ++i) any |= sig[i] > 0.f;
+    return any;
+}
+
+// Alpha compositing of one slab's 8 samples (forward/gaussians_aabb.cu:500-519).  A slab whose
+// samples all fell under the threshold composites to exactly nothing (alpha = 1 - exp(0) = 0).
 template <bool FAST>
 __device__ __forceinline__ void composite(RayState& r, const float* sig, const float3* C) {
+    if (!any_density(sig)) return;
 #pragma unroll
     for (int i = 0; i < kBuf; ++i) {
         if (FAST) {
+            // C[i] is zero wherever sig[i] is (both sum the same above-threshold samples)
             float alpha = 1.f - exp_neg<true>(sig[i] * kDt);
-            float3 c = C[i];
-            if (sig[i] > 0.f) c = c * (1.f / sig[i]);
-            r.C = r.C + c * (r.T * alpha);
+            float s = sig[i] > 0.f ? __fdividef(r.T * alpha, sig[i]) : 0.f;
+            r.C = r.C + C[i] * s;
             r.T *= 1.f - alpha;
         } else {
             float alpha = __fsub_rn(1.f, exp_neg<false>(__fmul_rn(sig[i], kDt)));
@@ -540,11 +554,11 @@ __device__ __forceinline__ float transpose_reduce16(float* v, int lane) {
 template <bool FAST, int CAP>
 __device__ __forceinline__ void slab_adjoint(const WarpSmem<FAST, CAP>& sm, int k, int K, bool has, const RayState& r,
                                              const RenderArgs& a, long long rgb_base, const float* roff,
-                                             const float* E, const float* F, const float* G, int lane,
+                                             const float* E, const float* F, const float* G, int nw, int lane,
                                              WarpStats& ws) {
     const int vid = ((lane >> 4) & 1) * 8 + ((lane >> 3) & 1) * 4 + ((lane >> 2) & 1) * 2 + ((lane >> 1) & 1);
 #pragma unroll 1
-    for (int w = 0; w < CAP / 32; ++w) {
+    for (int w = 0; w < nw; ++w) {
       unsigned mw = sm.smask[k / WarpSmem<FAST, CAP>::MB][w];
       while (mw) {
         const int e = 32 * w + __ffs(mw) - 1;
@@ -599,16 +613,17 @@ __device__ __forceinline__ void slab_adjoint(const WarpSmem<FAST, CAP>& sm, int 
                 float3 Smm = f3(m0.x * m0.x * U0 + 2.f * m0.x * mb.x * U1 + mb.x * mb.x * U2,
                                 m0.y * m0.y * U0 + 2.f * m0.y * mb.y * U1 + mb.y * mb.y * U2,
                                 m0.z * m0.z * U0 + 2.f * m0.z * mb.z * U1 + mb.z * mb.z * U2);
-                dsc = f3(Smm.x / s4.x, Smm.y / s4.y, Smm.z / s4.z);
+                const float3 is = f3(__fdividef(1.f, s4.x), __fdividef(1.f, s4.y), __fdividef(1.f, s4.z));
+                dsc = f3(Smm.x * is.x, Smm.y * is.y, Smm.z * is.z);
                 dp = f3(r0.x * Sm.x + r1.x * Sm.y + r2.x * Sm.z, r0.y * Sm.x + r1.y * Sm.y + r2.y * Sm.z,
                         r0.z * Sm.x + r1.z * Sm.y + r2.z * Sm.z);
                 // P[:, j] = sum_i u_i v_i m_ij with v_i = v0 + i vb, m_i = m0 + i mb
                 float3 P0 = v0 * (m0.x * U0 + mb.x * U1) + vb * (m0.x * U1 + mb.x * U2);
                 float3 P1 = v0 * (m0.y * U0 + mb.y * U1) + vb * (m0.y * U1 + mb.y * U2);
                 float3 P2 = v0 * (m0.z * U0 + mb.z * U1) + vb * (m0.z * U1 + mb.z * U2);
-                d1 = P0 * (-1.f / s4.x);
-                d2 = P1 * (-1.f / s4.y);
-                d3 = P2 * (-1.f / s4.z);
+                d1 = P0 * (-is.x);
+                d2 = P1 * (-is.y);
+                d3 = P2 * (-is.z);
             } else {
 #pragma unroll
                 for (int i = 0; i < kBuf; ++i) {
@@ -671,19 +686,27 @@ __device__ __forceinline__ void slab_adjoint_scalars(const RayState& r, const fl
     for (int i = 0; i < kBuf; ++i) {
         float cd = sig[i];
         float3 cc = Cb[i];
-        if (cd > 0.f) cc = cc * (1.f / cd);
+        float inv = 0.f;
+        if (cd > 0.f) {
+            inv = FAST ? __fdividef(1.f, cd) : 1.f / cd;
+            cc = cc * inv;
+        }
         float alpha = FAST ? 1.f - exp_neg<true>(cd * kDt) : __fsub_rn(1.f, exp_neg<false>(__fmul_rn(cd, kDt)));
         float3 aux = (cc * Ta - Ra) * kDt;
         E[i] = dot3(r.g, aux);
-        F[i] = cd > 0.f ? Ta * alpha / cd : 0.f;
+        F[i] = FAST ? Ta * alpha * inv : (cd > 0.f ? Ta * alpha / cd : 0.f);
         G[i] = dot3(r.g, cc);
         Ra = Ra - cc * (Ta * alpha);
         Ta = FAST ? Ta * (1.f - alpha) : __fmul_rn(Ta, __fsub_rn(1.f, alpha));
     }
 }
 
+#ifndef RG_FAST_MIN_BLOCKS
+#define RG_FAST_MIN_BLOCKS 0   // blocks per SM the fast kernels are compiled for (0: compiler choice)
+#endif
+
 template <bool BWD, bool FAST, int CAP>
-__global__ void __launch_bounds__(kWarpsPerBlock * 32) k_render(RenderArgs a) {
+__global__ void __launch_bounds__(kWarpsPerBlock * 32, FAST ? RG_FAST_MIN_BLOCKS : 0) k_render(RenderArgs a) {
     __shared__ WarpSmem<FAST, CAP> smem[kWarpsPerBlock];
     const int lane = threadIdx.x & 31;
     WarpSmem<FAST, CAP>& sm = smem[threadIdx.x >> 5];
@@ -823,7 +846,8 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32) k_render(RenderArgs a) {
                     float3 Cb[kBuf];
 #pragma unroll
                     for (int i = 0; i < kBuf; ++i) { sig[i] = 0.f; Cb[i] = f3(0.f, 0.f, 0.f); }
-                    int nh = slab_buffers<FAST, CAP>(sm, k, K, has, r, a, rgb_base, roff, sig, Cb, lane, ws);
+                    int nh =
+                        slab_buffers<FAST, CAP>(sm, k, K, has, r, a, rgb_base, roff, sig, Cb, nwords(count), lane, ws);
                     if (has) {
                         ++slabs_acc;
                         hits_acc += nh;
@@ -838,9 +862,9 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32) k_render(RenderArgs a) {
                         float E[kBuf], F[kBuf], G[kBuf], Ta;
                         float3 Ra;
                         slab_adjoint_scalars<FAST>(r, sig, Cb, E, F, G, Ta, Ra);
-                        bool act = has && nh > 0;
-                        slab_adjoint<FAST, CAP>(sm, k, K, act, r, a, rgb_base, roff, E, F, G, lane, ws);
-                        if (act) {
+                        bool act = has && nh > 0 && any_density(sig);
+                        slab_adjoint<FAST, CAP>(sm, k, K, act, r, a, rgb_base, roff, E, F, G, nwords(count), lane, ws);
+                        if (has && nh > 0) {
                             r.T = Ta;
                             r.C = Ra;
                             r.seed = seed_next;
@@ -862,14 +886,15 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32) k_render(RenderArgs a) {
                 float3 Cb[kBuf];
 #pragma unroll
                 for (int i = 0; i < kBuf; ++i) { sig[i] = 0.f; Cb[i] = f3(0.f, 0.f, 0.f); }
-                int nh = slab_buffers<FAST, CAP>(sm, 0, 1, has, r, a, rgb_base, roff, sig, Cb, lane, ws);
+                int nh = slab_buffers<FAST, CAP>(sm, 0, 1, has, r, a, rgb_base, roff, sig, Cb, nwords(count), lane, ws);
                 bool more = ovf;
                 while (more) {
                     int cursor = sm.ids[count - 1];
                     __syncwarp();
                     if (lane == 0) atomicAdd(&a.st->list_passes, 1ull);
                     count = traverse<FAST, CAP>(sm, a, r, on, seg_hi, 1, nv, cursor, more, lane, ws);
-                    nh += slab_buffers<FAST, CAP>(sm, 0, 1, has, r, a, rgb_base, roff, sig, Cb, lane, ws);
+                    nh += slab_buffers<FAST, CAP>(sm, 0, 1, has, r, a, rgb_base, roff, sig, Cb, nwords(count), lane,
+                                                  ws);
                 }
                 if (has) {
                     ++slabs_acc;
@@ -885,16 +910,16 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32) k_render(RenderArgs a) {
                     float E[kBuf], F[kBuf], G[kBuf], Ta;
                     float3 Ra;
                     slab_adjoint_scalars<FAST>(r, sig, Cb, E, F, G, Ta, Ra);
-                    bool act = has && nh > 0;
+                    bool act = has && nh > 0 && any_density(sig);
                     int cursor = -1;
                     bool more2 = true;
                     while (more2) {
                         count = traverse<FAST, CAP>(sm, a, r, on, seg_hi, 1, nv, cursor, more2, lane, ws);
-                        slab_adjoint<FAST, CAP>(sm, 0, 1, act, r, a, rgb_base, roff, E, F, G, lane, ws);
+                        slab_adjoint<FAST, CAP>(sm, 0, 1, act, r, a, rgb_base, roff, E, F, G, nwords(count), lane, ws);
                         if (more2) cursor = sm.ids[count - 1];
                         __syncwarp();
                     }
-                    if (act) {
+                    if (has && nh > 0) {
                         r.T = Ta;
                         r.C = Ra;
                         r.seed = seed_next;
