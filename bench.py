@@ -187,7 +187,7 @@ def our_arm(args, rank, world, local):
     tuning = eng.get_tuning()
     if not args.no_tune:
         from ray_gauss_b200.autotune import autotune
-        tuning = autotune(Pb, views, target, repeats=1, chunks=(32, 64, 128), capacities=(128,), ctas=(0,))
+        tuning = autotune(Pb, views, target, repeats=1, chunks=(32, 64, 128), capacities=(64,), ctas=(0,))
 
     # ---- headline: batched BF16-storage form (device-resident inputs) ----
     for _ in range(args.warmup):

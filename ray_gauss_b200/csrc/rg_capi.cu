@@ -28,7 +28,7 @@ struct rg_engine {
     long long n_built = -1;          // N of the last rg_bvh_build
     int colors_views = 0;            // views in the colour table
     rg_gaussians g_bbox{};           // parameters of the last rg_ellipsoids_bbox (borrowed pointers)
-    rg_tuning tuning{64, 0, 128, 0};
+    rg_tuning tuning{64, 0, 64, 0};
     unsigned long long launches = 0;
     char last_err[256] = {0};
 };

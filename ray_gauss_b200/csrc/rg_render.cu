@@ -585,13 +585,17 @@ __device__ __forceinline__ void slab_adjoint(const WarpSmem<FAST, CAP>& sm, int 
             float gc = 0.f, dd = 0.f;
             float3 dsc = f3(0.f, 0.f, 0.f), dp = f3(0.f, 0.f, 0.f);
             float3 d1 = f3(0.f, 0.f, 0.f), d2 = f3(0.f, 0.f, 0.f), d3 = f3(0.f, 0.f, 0.f);
+            // Moment form: with sample positions v_i = v0 + x_i vb and m_i = m0 + x_i mb, every
+            // gradient is linear in U_k = sum_i u_i x_i^k (k = 0, 1, 2), u_i = dens * h_i * w_i.
+            // Fast arithmetic: x_i = i, vb = dt * dir.  Parity: x_i = t_i - tb, vb = dir (random
+            // sample offsets included); its weights and threshold decisions are the reference's.
+            const float3 v0 = (r.o + r.d * r.tb) - mu;
+            const float3 vb = FAST ? r.d * kDt : r.d;
+            const float3 m0 = f3(dot3(r0, v0), dot3(r1, v0), dot3(r2, v0));
+            const float3 mb = f3(dot3(r0, vb), dot3(r1, vb), dot3(r2, vb));
+            float U0 = 0.f, U1 = 0.f, U2 = 0.f;
             if (FAST) {
-                float3 v0 = (r.o + r.d * r.tb) - mu;
-                float3 vb = r.d * kDt;
-                float3 m0 = f3(dot3(r0, v0), dot3(r1, v0), dot3(r2, v0));
-                float3 mb = f3(dot3(r0, vb), dot3(r1, vb), dot3(r2, vb));
                 float A = dot3(m0, m0), B2 = 2.f * dot3(m0, mb), Cq = dot3(mb, mb);
-                float U0 = 0.f, U1 = 0.f, U2 = 0.f;
 #pragma unroll
                 for (int i = 0; i < kBuf; ++i) {
                     float fi = (float)i;
@@ -607,23 +611,6 @@ __device__ __forceinline__ void slab_adjoint(const WarpSmem<FAST, CAP>& sm, int 
                         U2 += fi * fi * u;
                     }
                 }
-                gc *= dn;
-                U0 *= dn; U1 *= dn; U2 *= dn;
-                float3 Sm = m0 * U0 + mb * U1;
-                float3 Smm = f3(m0.x * m0.x * U0 + 2.f * m0.x * mb.x * U1 + mb.x * mb.x * U2,
-                                m0.y * m0.y * U0 + 2.f * m0.y * mb.y * U1 + mb.y * mb.y * U2,
-                                m0.z * m0.z * U0 + 2.f * m0.z * mb.z * U1 + mb.z * mb.z * U2);
-                const float3 is = f3(__fdividef(1.f, s4.x), __fdividef(1.f, s4.y), __fdividef(1.f, s4.z));
-                dsc = f3(Smm.x * is.x, Smm.y * is.y, Smm.z * is.z);
-                dp = f3(r0.x * Sm.x + r1.x * Sm.y + r2.x * Sm.z, r0.y * Sm.x + r1.y * Sm.y + r2.y * Sm.z,
-                        r0.z * Sm.x + r1.z * Sm.y + r2.z * Sm.z);
-                // P[:, j] = sum_i u_i v_i m_ij with v_i = v0 + i vb, m_i = m0 + i mb
-                float3 P0 = v0 * (m0.x * U0 + mb.x * U1) + vb * (m0.x * U1 + mb.x * U2);
-                float3 P1 = v0 * (m0.y * U0 + mb.y * U1) + vb * (m0.y * U1 + mb.y * U2);
-                float3 P2 = v0 * (m0.z * U0 + mb.z * U1) + vb * (m0.z * U1 + mb.z * U2);
-                d1 = P0 * (-is.x);
-                d2 = P1 * (-is.y);
-                d3 = P2 * (-is.z);
             } else {
 #pragma unroll
                 for (int i = 0; i < kBuf; ++i) {
@@ -633,20 +620,35 @@ __device__ __forceinline__ void slab_adjoint(const WarpSmem<FAST, CAP>& sm, int 
                     float wt = parity_weight(r.o, r.d, t, mu, r0, r1, r2, dn, vv, m, in);
                     if (in) {
                         float h = E[i] + F[i] * (gcol - G[i]);
-                        gc += wt * dn * F[i];
+                        gc += wt * F[i];
                         dd += wt * h;
-                        float u = dn * h * wt;
-                        dsc.x += u * (m.x * m.x) / s4.x;
-                        dsc.y += u * (m.y * m.y) / s4.y;
-                        dsc.z += u * (m.z * m.z) / s4.z;
-                        dp.x += u * (r0.x * m.x + r1.x * m.y + r2.x * m.z);
-                        dp.y += u * (r0.y * m.x + r1.y * m.y + r2.y * m.z);
-                        dp.z += u * (r0.z * m.x + r1.z * m.y + r2.z * m.z);
-                        d1 = d1 - vv * (u * m.x / s4.x);
-                        d2 = d2 - vv * (u * m.y / s4.y);
-                        d3 = d3 - vv * (u * m.z / s4.z);
+                        float u = h * wt;
+                        float x = t - r.tb;
+                        U0 += u;
+                        U1 += x * u;
+                        U2 += x * x * u;
                     }
                 }
+            }
+            {
+                gc *= dn;
+                U0 *= dn; U1 *= dn; U2 *= dn;
+                float3 Sm = m0 * U0 + mb * U1;
+                float3 Smm = f3(m0.x * m0.x * U0 + 2.f * m0.x * mb.x * U1 + mb.x * mb.x * U2,
+                                m0.y * m0.y * U0 + 2.f * m0.y * mb.y * U1 + mb.y * mb.y * U2,
+                                m0.z * m0.z * U0 + 2.f * m0.z * mb.z * U1 + mb.z * mb.z * U2);
+                const float3 is = FAST ? f3(__fdividef(1.f, s4.x), __fdividef(1.f, s4.y), __fdividef(1.f, s4.z))
+                                       : f3(1.f / s4.x, 1.f / s4.y, 1.f / s4.z);
+                dsc = f3(Smm.x * is.x, Smm.y * is.y, Smm.z * is.z);
+                dp = f3(r0.x * Sm.x + r1.x * Sm.y + r2.x * Sm.z, r0.y * Sm.x + r1.y * Sm.y + r2.y * Sm.z,
+                        r0.z * Sm.x + r1.z * Sm.y + r2.z * Sm.z);
+                // P[:, j] = sum_i u_i v_i m_ij
+                float3 P0 = v0 * (m0.x * U0 + mb.x * U1) + vb * (m0.x * U1 + mb.x * U2);
+                float3 P1 = v0 * (m0.y * U0 + mb.y * U1) + vb * (m0.y * U1 + mb.y * U2);
+                float3 P2 = v0 * (m0.z * U0 + mb.z * U1) + vb * (m0.z * U1 + mb.z * U2);
+                d1 = P0 * (-is.x);
+                d2 = P1 * (-is.y);
+                d3 = P2 * (-is.z);
             }
             float4 dq = quat_grad(q4, d1, d2, d3);
             v[0] = dd; v[1] = dp.x; v[2] = dp.y; v[3] = dp.z;
@@ -701,12 +703,29 @@ __device__ __forceinline__ void slab_adjoint_scalars(const RayState& r, const fl
     }
 }
 
-#ifndef RG_FAST_MIN_BLOCKS
-#define RG_FAST_MIN_BLOCKS 0   // blocks per SM the fast kernels are compiled for (0: compiler choice)
+// Resident blocks per SM each kernel is compiled for (0: the compiler's choice).  The defaults
+// fit the shared memory of the 64-entry tuning (256-entry fast lists) and were measured best on
+// 1M Gaussians x 16 views.
+#ifndef RG_FAST_FWD_MIN_BLOCKS
+#define RG_FAST_FWD_MIN_BLOCKS 7
 #endif
+#ifndef RG_FAST_BWD_MIN_BLOCKS
+#define RG_FAST_BWD_MIN_BLOCKS 7
+#endif
+#ifndef RG_PAR_FWD_MIN_BLOCKS
+#define RG_PAR_FWD_MIN_BLOCKS 5
+#endif
+#ifndef RG_PAR_BWD_MIN_BLOCKS
+#define RG_PAR_BWD_MIN_BLOCKS 5
+#endif
+template <bool BWD, bool FAST>
+constexpr int min_blocks() {
+    return FAST ? (BWD ? RG_FAST_BWD_MIN_BLOCKS : RG_FAST_FWD_MIN_BLOCKS)
+                : (BWD ? RG_PAR_BWD_MIN_BLOCKS : RG_PAR_FWD_MIN_BLOCKS);
+}
 
 template <bool BWD, bool FAST, int CAP>
-__global__ void __launch_bounds__(kWarpsPerBlock * 32, FAST ? RG_FAST_MIN_BLOCKS : 0) k_render(RenderArgs a) {
+__global__ void __launch_bounds__(kWarpsPerBlock * 32, min_blocks<BWD, FAST>()) k_render(RenderArgs a) {
     __shared__ WarpSmem<FAST, CAP> smem[kWarpsPerBlock];
     const int lane = threadIdx.x & 31;
     WarpSmem<FAST, CAP>& sm = smem[threadIdx.x >> 5];
