@@ -35,7 +35,7 @@
 extern "C" {
 #endif
 
-#define RG_ABI_VERSION 1
+#define RG_ABI_VERSION 2
 
 #if defined(__GNUC__)
 #define RG_API __attribute__((visibility("default")))
@@ -137,6 +137,9 @@ typedef struct rg_status {
     uint64_t list_entries;             /* warp hit-list entries appended */
     uint64_t slab_steps;               /* warp-level slab iterations with at least one entry */
     uint64_t entry_slabs;              /* warp-level (entry, slab) evaluations */
+    uint64_t replayed_chunks;          /* backward chunks replayed from the forward's hit-list record */
+    uint64_t record_overflows;         /* tiles whose hit-list record did not fit (backward traverses) */
+    uint64_t record_words;             /* 4-byte words of the last forward's hit-list record */
 } rg_status;
 
 /* Kernel tuning knobs (rg_autotune picks them; 0 = keep the current value). */
@@ -144,7 +147,8 @@ typedef struct rg_tuning {
     int32_t chunk_slabs;               /* longest traversal chunk in slabs, 1..255 */
     int32_t blocks_per_sm;             /* resident render CTAs per SM */
     int32_t list_capacity;             /* warp hit-list capacity: 64 or 128 */
-    int32_t reserved;
+    int32_t record_hits;               /* 1: the forward records its hit lists and the backward
+                                          replays them (default); -1: the backward traverses */
 } rg_tuning;
 
 typedef struct rg_engine rg_engine;
@@ -153,7 +157,8 @@ typedef struct rg_engine rg_engine;
 RG_API int rg_create(rg_engine** out, int device);
 RG_API int rg_destroy(rg_engine* e);
 /* Size the engine's scratch for n Gaussians, up to n_views views and n_rays rays per call.
- * Calls made afterwards with sizes within these bounds allocate nothing. */
+ * Calls made afterwards with sizes within these bounds allocate nothing.  n_rays also sizes the
+ * hit-list record (96 B per ray); without it the backward traverses the BVH again. */
 RG_API int rg_reserve(rg_engine* e, int64_t n, int32_t n_views, int64_t n_rays);
 RG_API int rg_set_tuning(rg_engine* e, const rg_tuning* t);
 RG_API int rg_get_tuning(const rg_engine* e, rg_tuning* t);
@@ -178,8 +183,10 @@ RG_API int rg_forward_sh(rg_engine* e, const rg_gaussians* g, const rg_camera* c
  * views' rays packed in order, ray y*W+x within a view; final_T (R,) optional. */
 RG_API int rg_launch_forward(rg_engine* e, const rg_camera* cams, int32_t n_cams, const rg_settings* s,
                       float* ray_colors, float* final_T, void* stream);
-/* optix_utils.py:213-299: re-traverse and scatter per-Gaussian gradients into the engine's
- * accumulators (zeroed by this call).  ray_colors are the forward outputs. */
+/* optix_utils.py:213-299: recompute the forward's slabs and scatter per-Gaussian gradients into
+ * the engine's accumulators (zeroed by this call).  ray_colors are the forward outputs.  When no
+ * bbox/BVH/colour/tuning call came after the last rg_launch_forward and cams, n_cams and *s are
+ * that forward's, its recorded warp hit lists are replayed instead of traversing the BVH again. */
 RG_API int rg_launch_backward(rg_engine* e, const rg_camera* cams, int32_t n_cams, const rg_settings* s,
                        const float* ray_colors, const float* dloss_dray_colors, void* stream);
 /* utils/sh_utils.cu:121-315 + render_optix.py:170-190: SH/SG backward for every view and the

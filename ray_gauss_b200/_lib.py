@@ -56,12 +56,13 @@ class rg_status(ctypes.Structure):
     _fields_ = [(k, ctypes.c_uint64) for k in ("hit_pairs", "slabs", "slab_cap_exceeded", "list_passes",
                                                 "chunk_splits", "stack_overflows", "watchdog_trips",
                                                 "nonfinite_inputs", "traversals", "node_visits", "leaf_tests",
-                                                "list_entries", "slab_steps", "entry_slabs")]
+                                                "list_entries", "slab_steps", "entry_slabs", "replayed_chunks",
+                                                "record_overflows", "record_words")]
 
 
 class rg_tuning(ctypes.Structure):
     _fields_ = [("chunk_slabs", ctypes.c_int32), ("blocks_per_sm", ctypes.c_int32),
-                ("list_capacity", ctypes.c_int32), ("reserved", ctypes.c_int32)]
+                ("list_capacity", ctypes.c_int32), ("record_hits", ctypes.c_int32)]
 
 
 assert ctypes.sizeof(rg_camera) == 64
@@ -116,7 +117,7 @@ def load(path: str = LIB_PATH):
             fn = getattr(lib, name)
             fn.restype = res
             fn.argtypes = args
-        if lib.rg_abi_version() != 1:
+        if lib.rg_abi_version() != 2:
             raise RuntimeError("raygauss_b200 ABI version mismatch")
         _LIB = lib
         return lib

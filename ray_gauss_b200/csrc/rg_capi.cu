@@ -1,5 +1,6 @@
 // C ABI of the engine (include/raygauss_b200.h): argument validation, scratch ownership and the
 // stream-ordered launch sequences of the reference's forward and backward.
+#include <algorithm>
 #include <climits>
 #include <cstdio>
 #include <cstring>
@@ -28,7 +29,17 @@ struct rg_engine {
     long long n_built = -1;          // N of the last rg_bvh_build
     int colors_views = 0;            // views in the colour table
     rg_gaussians g_bbox{};           // parameters of the last rg_ellipsoids_bbox (borrowed pointers)
-    rg_tuning tuning{64, 0, 64, 0};
+    // hit-list record of the last forward (replayed by the backward of the same launch)
+    unsigned* rec_arena = nullptr;
+    unsigned long long* rec_top = nullptr;
+    unsigned rec_cap = 0;            // arena words
+    unsigned* rec_tile = nullptr;
+    int rec_tiles = 0;
+    bool rec_valid = false;          // the arena holds the record of the launch described below
+    const rg_camera* rec_cams = nullptr;
+    int rec_n_cams = 0;
+    rg_settings rec_settings{};
+    rg_tuning tuning{64, 0, 64, 1};
     unsigned long long launches = 0;
     char last_err[256] = {0};
 };
@@ -101,6 +112,29 @@ int ensure_views(rg_engine* e, int views) {
     if ((rc = grow(e, e->gacc_rgb, N * (size_t)views))) return rc;
     e->cap_views = views;
     e->colors_views = 0;
+    return RG_OK;
+}
+
+constexpr long long kRecordWordsPerRay = 24;
+constexpr long long kRecordBaseWords = 4096;
+
+// Hit-list record storage for launches of up to n_rays rays (tiles <= rays).
+int ensure_record(rg_engine* e, long long n_rays) {
+    long long words = std::min(n_rays * kRecordWordsPerRay + kRecordBaseWords, (long long)0xfffffff0ll);
+    long long tiles = std::min(n_rays, (long long)INT_MAX);
+    int rc;
+    if (!e->rec_top && (rc = grow(e, e->rec_top, 1))) return rc;
+    if (words > (long long)e->rec_cap) {
+        e->rec_cap = 0;
+        if ((rc = grow(e, e->rec_arena, (size_t)words))) return rc;
+        e->rec_cap = (unsigned)words;
+    }
+    if (tiles > e->rec_tiles) {
+        e->rec_tiles = 0;
+        if ((rc = grow(e, e->rec_tile, (size_t)tiles))) return rc;
+        e->rec_tiles = (int)tiles;
+    }
+    e->rec_valid = false;
     return RG_OK;
 }
 
@@ -207,7 +241,8 @@ int rg_destroy(rg_engine* e) {
     void* ptrs[] = {e->rec, e->aabb, e->scene_ord, e->bvh.keys_in, e->bvh.keys_out, e->bvh.vals_in, e->bvh.leaf_gid,
                     e->bvh.rank, e->bvh.leaf_rec, e->bvh.leaf_is, e->bvh.leaf_ext, e->bvh.leaf_lo, e->bvh.leaf_hi, e->bvh.nodes,
                     e->bvh.leaf_parent, e->bvh.node_parent, e->bvh.refit_cnt, e->bvh.root_box, e->bvh.sort_temp,
-                    e->rgb_leaf, e->gacc_geo, e->gacc_rgb, e->vt, e->work_counter, e->st};
+                    e->rgb_leaf, e->gacc_geo, e->gacc_rgb, e->vt, e->work_counter, e->st, e->rec_arena,
+                    e->rec_top, e->rec_tile};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     delete e;
@@ -220,7 +255,10 @@ int rg_reserve(rg_engine* e, int64_t n, int32_t n_views, int64_t n_rays) {
     if (rc) return rc;
     if (n > 0 && (rc = ensure_n(e, n))) return rc;
     if (n_views > 0 && (rc = ensure_views(e, n_views))) return rc;
-    if (n_rays > e->cap_rays) e->cap_rays = n_rays;
+    if (n_rays > e->cap_rays) {
+        if ((rc = ensure_record(e, n_rays))) return rc;
+        e->cap_rays = n_rays;
+    }
     return RG_OK;
 }
 
@@ -230,9 +268,12 @@ int rg_set_tuning(rg_engine* e, const rg_tuning* t) {
     if (t->list_capacity != 0 && t->list_capacity != 64 && t->list_capacity != 128)
         return RG_ERR_INVALID_ARG;
     if (t->blocks_per_sm < 0) return RG_ERR_INVALID_ARG;
+    if (t->record_hits < -1 || t->record_hits > 1) return RG_ERR_INVALID_ARG;
     if (t->chunk_slabs) e->tuning.chunk_slabs = t->chunk_slabs;
     if (t->list_capacity) e->tuning.list_capacity = t->list_capacity;
+    if (t->record_hits) e->tuning.record_hits = t->record_hits;
     e->tuning.blocks_per_sm = t->blocks_per_sm;
+    e->rec_valid = false;
     return RG_OK;
 }
 
@@ -260,6 +301,7 @@ int rg_ellipsoids_bbox(rg_engine* e, const rg_gaussians* g, float* aabb_out, flo
     }
     e->n_bbox = g->n;
     e->g_bbox = *g;
+    e->rec_valid = false;
     return RG_OK;
 }
 
@@ -274,6 +316,7 @@ int rg_bvh_build(rg_engine* e, void* stream) {
     e->launches += 6;
     e->n_built = e->n_bbox;
     e->colors_views = 0;
+    e->rec_valid = false;
     return RG_OK;
 }
 
@@ -285,6 +328,7 @@ int rg_bvh_refit(rg_engine* e, void* stream) {
     RG_CUDA(rg::launch_refit(e->n_built, e->aabb, e->rec, g, e->bvh, S(stream)), "bvh refit");
     e->launches += 2;
     e->colors_views = 0;
+    e->rec_valid = false;
     return RG_OK;
 }
 
@@ -299,6 +343,7 @@ int rg_forward_sh(rg_engine* e, const rg_gaussians* g, const rg_camera* cams, in
     RG_CUDA(rg::launch_color_forward(g, cams, n_cams, e->bvh.rank, e->rgb_leaf, rgb_out, S(stream)), "forward_sh");
     e->launches += 1;
     e->colors_views = n_cams;
+    e->rec_valid = false;
     return RG_OK;
 }
 
@@ -314,9 +359,25 @@ int rg_launch_forward(rg_engine* e, const rg_camera* cams, int32_t n_cams, const
     fill_args(e, cams, s, a);
     a.ray_colors = ray_colors;
     a.final_T = final_T;
+    const bool record = e->tuning.record_hits == 1 && e->rec_arena != nullptr;
+    e->rec_valid = false;
+    if (record) {
+        RG_CUDA(cudaMemsetAsync(e->rec_top, 0, sizeof(unsigned long long), S(stream)), "reset record");
+        a.rec_arena = e->rec_arena;
+        a.rec_top = e->rec_top;
+        a.rec_cap = e->rec_cap;
+        a.rec_tile = e->rec_tile;
+        a.rec_tiles = e->rec_tiles;
+    }
     int grid = render_grid(e, false, s->mode);
     RG_CUDA(rg::launch_render(false, s->mode, e->tuning.list_capacity, grid, a, S(stream)), "render forward");
     e->launches += 2;
+    if (record) {
+        e->rec_valid = true;
+        e->rec_cams = cams;
+        e->rec_n_cams = n_cams;
+        e->rec_settings = *s;
+    }
     return RG_OK;
 }
 
@@ -337,6 +398,17 @@ int rg_launch_backward(rg_engine* e, const rg_camera* cams, int32_t n_cams, cons
     a.dL = dloss_dray_colors;
     a.gacc_geo = e->gacc_geo;
     a.gacc_rgb = e->gacc_rgb;
+    // Replay the last forward's hit lists when nothing changed the engine state since that forward
+    // (bbox, BVH, colour and tuning calls invalidate the record) and this backward uses the same
+    // camera table, view count and settings: the chunk sequence is then the forward's.
+    if (e->rec_valid && e->tuning.record_hits == 1 && e->rec_cams == cams && e->rec_n_cams == n_cams &&
+        std::memcmp(&e->rec_settings, s, sizeof(rg_settings)) == 0) {
+        a.rec_arena = e->rec_arena;
+        a.rec_cap = e->rec_cap;
+        a.rec_tile = e->rec_tile;
+        a.rec_tiles = e->rec_tiles;
+        a.replay = 1;
+    }
     int grid = render_grid(e, true, s->mode);
     RG_CUDA(rg::launch_render(true, s->mode, e->tuning.list_capacity, grid, a, S(stream)), "render backward");
     e->launches += 2;
@@ -413,6 +485,14 @@ int rg_get_status(rg_engine* e, rg_status* out, int32_t reset, void* stream) {
     out->list_entries = h.list_entries;
     out->slab_steps = h.slab_steps;
     out->entry_slabs = h.entry_slabs;
+    out->replayed_chunks = h.replayed_chunks;
+    out->record_overflows = h.record_overflows;
+    out->record_words = 0;
+    if (e->rec_top) {
+        unsigned long long w = 0;
+        RG_CUDA(cudaMemcpy(&w, e->rec_top, sizeof(w), cudaMemcpyDeviceToHost), "read record size");
+        out->record_words = w;
+    }
     if (reset) RG_CUDA(cudaMemset(e->st, 0, sizeof(rg::DevStatus)), "reset status");
     return RG_OK;
 }

@@ -38,6 +38,8 @@ struct DevStatus {
     unsigned long long list_entries;      // hit-list entries appended
     unsigned long long slab_steps;        // warp-level slab iterations with at least one entry
     unsigned long long entry_slabs;       // warp-level (entry, slab) evaluations
+    unsigned long long replayed_chunks;   // backward chunks whose list came from the forward record
+    unsigned long long record_overflows;  // tiles whose record did not fit the arena
 };
 
 // Per-launch view table computed on the device from the camera array (no host sync).
@@ -81,6 +83,12 @@ __device__ __forceinline__ float load_param(const void* p, long long i, int stor
 __device__ __forceinline__ float ex2_approx(float x) {
     float y;
     asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+// SFU base-2 logarithm (x <= 0 gives -inf / NaN, which fail every threshold comparison)
+__device__ __forceinline__ float lg2_approx(float x) {
+    float y;
+    asm("lg2.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
     return y;
 }
 

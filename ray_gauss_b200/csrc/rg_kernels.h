@@ -48,6 +48,14 @@ struct RenderArgs {
     float4* gacc_rgb;             // (n_views, n_leaves): {drgb.xyz, 0}
     int* work_counter;
     DevStatus* st;
+    // hit-list record: the forward appends each warp chunk's leaf ids to the arena (chunk records
+    // linked per tile); the backward replays them instead of traversing.  Null arena: no record.
+    unsigned* rec_arena;
+    unsigned long long* rec_top;  // words used (reset before every recording forward)
+    unsigned rec_cap;             // arena words
+    unsigned* rec_tile;           // first chunk record of each tile (kNoRecord: none)
+    int rec_tiles;                // entries of rec_tile
+    int replay;                   // backward: replay the records
 };
 
 cudaError_t launch_prepass(const rg_gaussians* g, GaussRec* rec, float* aabb, int* scene_ord, DevStatus* st,

@@ -42,8 +42,12 @@ constexpr int kWarpsPerBlock = 4;
 constexpr unsigned kFull = 0xffffffffu;
 constexpr int kMaxRounds = 1 << 20;        // chunk rounds per tile before the watchdog trips
 constexpr float kNegHalfLog2e = -0.72134752044448170f;
+constexpr float kLog2SigThr = -3.3219280948873623f;   // log2(0.1): per-sample density threshold
 constexpr float kInvSlab = 50.0f;          // 1 / 0.02
 constexpr int kExactChunk = 8;             // chunks up to this length use exact slab ranges
+constexpr unsigned kNoRecord = 0xffffffffu;     // hit-list record: no (next) chunk record
+constexpr unsigned kRecordMulti = 0x80000000u;  // chunk consumed in several traversal passes
+constexpr unsigned kRecordFailed = 0xfffffffeu; // the tile's record did not fit the arena
 
 // Warp hit-list layout.  Parity arithmetic keeps, per entry and lane, the exact range of the
 // chunk's slabs the lane's interval covers (64 B per entry); the fast arithmetic keeps only the mask
@@ -63,16 +67,20 @@ struct WarpSmem {
     unsigned smask[NB][CAP / 32];                    // entries whose union range meets block k / MB
     unsigned long long occ[4];                       // slabs holding any entry (union occupancy)
     int stack[kStack];
+    // hit-list record of the warp's current tile (written by lane 0)
+    unsigned rec_first, rec_prev;                    // forward: first / last chunk record
+    unsigned rec_cur;                                // backward: next chunk record to replay
 };
 
 // Warp-uniform activity counters (flushed once per warp).
 struct WarpStats {
     unsigned long long traversals = 0, node_visits = 0, leaf_tests = 0, entries = 0, slab_steps = 0,
-                       entry_slabs = 0;
+                       entry_slabs = 0, replays = 0;
 };
 
 struct RayState {
     float3 o, d, invd;
+    float3 oid;   // -o * invd (fast box test)
     float tenter, texit;
     float tb;
     float T;
@@ -90,10 +98,21 @@ __device__ __forceinline__ float3 rows_rn(float3 r0, float3 r1, float3 r2, float
     return f3(dot_rn(r0, v), dot_rn(r1, v), dot_rn(r2, v));
 }
 
+// Slab test of a BVH box against [lo, hi].  The fast arithmetic evaluates t = b/d - o/d with one
+// FMA per plane; its rounding (~1e-7 of |o/d|) stays inside the leaf boxes' 1e-5 inflation for
+// scenes within a few hundred units of the camera.
+template <bool FAST>
 __device__ __forceinline__ bool box_hit(const float* bx, const RayState& r, float lo, float hi) {
-    float tx0 = (bx[0] - r.o.x) * r.invd.x, tx1 = (bx[3] - r.o.x) * r.invd.x;
-    float ty0 = (bx[1] - r.o.y) * r.invd.y, ty1 = (bx[4] - r.o.y) * r.invd.y;
-    float tz0 = (bx[2] - r.o.z) * r.invd.z, tz1 = (bx[5] - r.o.z) * r.invd.z;
+    float tx0, tx1, ty0, ty1, tz0, tz1;
+    if (FAST) {
+        tx0 = fmaf(bx[0], r.invd.x, r.oid.x); tx1 = fmaf(bx[3], r.invd.x, r.oid.x);
+        ty0 = fmaf(bx[1], r.invd.y, r.oid.y); ty1 = fmaf(bx[4], r.invd.y, r.oid.y);
+        tz0 = fmaf(bx[2], r.invd.z, r.oid.z); tz1 = fmaf(bx[5], r.invd.z, r.oid.z);
+    } else {
+        tx0 = (bx[0] - r.o.x) * r.invd.x; tx1 = (bx[3] - r.o.x) * r.invd.x;
+        ty0 = (bx[1] - r.o.y) * r.invd.y; ty1 = (bx[4] - r.o.y) * r.invd.y;
+        tz0 = (bx[2] - r.o.z) * r.invd.z; tz1 = (bx[5] - r.o.z) * r.invd.z;
+    }
     float tn = fmaxf(fmaxf(lo, fminf(tx0, tx1)), fmaxf(fminf(ty0, ty1), fminf(tz0, tz1)));
     float tf = fminf(fminf(hi, fmaxf(tx0, tx1)), fminf(fmaxf(ty0, ty1), fmaxf(tz0, tz1)));
     return tn <= tf;
@@ -230,6 +249,76 @@ __device__ __forceinline__ int occ_next(const unsigned long long* occ, int k, in
     return K;
 }
 
+// Exact leaf test of every active lane for the chunk [tb, seg_hi]: appends the leaf to the warp
+// list when any lane's interval meets one of the chunk's slabs.  Returns false (leaf not taken)
+// when the list is already full.
+template <bool FAST, int CAP>
+__device__ __forceinline__ bool leaf_entry(WarpSmem<FAST, CAP>& sm, const RenderArgs& a, const RayState& r, bool on,
+                                           float seg_hi, int K, int nv, int leaf, int& count,
+                                           unsigned long long* occ, int lane, WarpStats& ws) {
+    ++ws.leaf_tests;
+    int lo = 255, hi = -1;
+    if (on) {
+        float root1, root2;
+        bool ok;
+        if (FAST) {
+            ok = roots_fast(load_rec(a.rec, leaf), r, root1, root2);
+        } else {
+            float4 m4 = __ldg(reinterpret_cast<const float4*>(a.rec + leaf));
+            ok = roots_exact(load_is(a.is_rec, leaf), f3(m4.x, m4.y, m4.z), r, root1, root2);
+        }
+        if (ok) slab_range(r, K, nv, seg_hi, root1, root2, lo, hi);
+    }
+    unsigned any = __ballot_sync(kFull, lo <= hi);
+    if (!any) return true;
+    if (count == CAP) return false;
+    int ulo = (int)__reduce_min_sync(kFull, (unsigned)lo);
+    int uhi = (int)__reduce_max_sync(kFull, (unsigned)(hi + 1)) - 1;
+    if (FAST) {
+        if (lane == 0) sm.lmask[count] = any;
+    } else {
+        sm.lrng[count][lane] = (unsigned short)((lo & 0xff) | ((hi & 0xff) << 8));
+    }
+    if (lane == 0) {
+        sm.ids[count] = leaf;
+        sm.urng[count] = (unsigned)ulo | ((unsigned)uhi << 16);
+    }
+    occ_set(occ, ulo, uhi);
+    ++count;
+    return true;
+}
+
+// Publishes the chunk list: occupancy bits and the entry masks per block of MB slabs.
+template <bool FAST, int CAP>
+__device__ __forceinline__ void finish_list(WarpSmem<FAST, CAP>& sm, int count, int K, const unsigned long long* occ,
+                                            int lane, WarpStats& ws) {
+    __syncwarp();
+    if (lane == 0) {
+#pragma unroll
+        for (int w = 0; w < 4; ++w) sm.occ[w] = occ[w];
+    }
+    ws.entries += count;
+    // lane l fills blocks l, l+32
+    constexpr int MB = WarpSmem<FAST, CAP>::MB;
+    const int nblk = (K + MB - 1) / MB;
+    const int nw = nwords(count);
+    for (int bk = lane; bk < nblk; bk += 32) {
+        const int k0 = bk * MB, k1 = k0 + MB - 1;
+#pragma unroll 1
+        for (int w = 0; w < nw; ++w) {
+            unsigned mw = 0u;
+            const int e0 = 32 * w, e1 = min(count, e0 + 32);
+#pragma unroll 1
+            for (int e = e0; e < e1; ++e) {
+                unsigned u = sm.urng[e];
+                if (k1 >= (int)(u & 0xffff) && k0 <= (int)(u >> 16)) mw |= 1u << (e - e0);
+            }
+            sm.smask[bk][w] = mw;
+        }
+    }
+    __syncwarp();
+}
+
 // Warp-cooperative traversal for the chunk [tb, seg_hi] of every active lane.  Appends hit leaves
 // with index > cursor to the warp list; returns the entry count.  `ovf` is set when the list
 // filled up before the traversal finished.
@@ -256,8 +345,8 @@ __device__ int traverse(WarpSmem<FAST, CAP>& sm, const RenderArgs& a, const RayS
             int4 n3 = __ldg(reinterpret_cast<const int4*>(np + 3));
             float lb[6] = {n0.x, n0.y, n0.z, n0.w, n1.x, n1.y};
             float rb[6] = {n1.z, n1.w, n2.x, n2.y, n2.z, n2.w};
-            bool hl = on && n3.z > cursor && box_hit(lb, r, r.tb, seg_hi);
-            bool hr = on && n3.w > cursor && box_hit(rb, r, r.tb, seg_hi);
+            bool hl = on && n3.z > cursor && box_hit<FAST>(lb, r, r.tb, seg_hi);
+            bool hr = on && n3.w > cursor && box_hit<FAST>(rb, r, r.tb, seg_hi);
             unsigned bl = __ballot_sync(kFull, hl), br = __ballot_sync(kFull, hr);
             if (bl && br) {
                 if (sp < kStack) {
@@ -274,71 +363,38 @@ __device__ int traverse(WarpSmem<FAST, CAP>& sm, const RenderArgs& a, const RayS
             if (br) { cur = n3.y; continue; }
         } else {
             int leaf = ~cur;
-            if (leaf > cursor) {
-                ++ws.leaf_tests;
-                int lo = 255, hi = -1;
-                if (on) {
-                    float root1, root2;
-                    bool ok;
-                    if (FAST) {
-                        ok = roots_fast(load_rec(a.rec, leaf), r, root1, root2);
-                    } else {
-                        float4 m4 = __ldg(reinterpret_cast<const float4*>(a.rec + leaf));
-                        ok = roots_exact(load_is(a.is_rec, leaf), f3(m4.x, m4.y, m4.z), r, root1, root2);
-                    }
-                    if (ok) slab_range(r, K, nv, seg_hi, root1, root2, lo, hi);
-                }
-                unsigned any = __ballot_sync(kFull, lo <= hi);
-                if (any) {
-                    if (count == CAP) {
-                        ovf = true;
-                        break;
-                    }
-                    int ulo = (int)__reduce_min_sync(kFull, (unsigned)lo);
-                    int uhi = (int)__reduce_max_sync(kFull, (unsigned)(hi + 1)) - 1;
-                    if (FAST) {
-                        if (lane == 0) sm.lmask[count] = any;
-                    } else {
-                        sm.lrng[count][lane] = (unsigned short)((lo & 0xff) | ((hi & 0xff) << 8));
-                    }
-                    if (lane == 0) {
-                        sm.ids[count] = leaf;
-                        sm.urng[count] = (unsigned)ulo | ((unsigned)uhi << 16);
-                    }
-                    occ_set(occ, ulo, uhi);
-                    ++count;
-                }
+            if (leaf > cursor && !leaf_entry<FAST, CAP>(sm, a, r, on, seg_hi, K, nv, leaf, count, occ, lane, ws)) {
+                ovf = true;
+                break;
             }
         }
         if (sp == 0) break;
         __syncwarp();
         cur = sm.stack[--sp];
     }
-    __syncwarp();
-    if (lane == 0) {
-#pragma unroll
-        for (int w = 0; w < 4; ++w) sm.occ[w] = occ[w];
-    }
-    ws.entries += count;
-    // entry masks per block of MB slabs: lane l fills blocks l, l+32
-    constexpr int MB = WarpSmem<FAST, CAP>::MB;
-    const int nblk = (K + MB - 1) / MB;
-    const int nw = nwords(count);
-    for (int bk = lane; bk < nblk; bk += 32) {
-        const int k0 = bk * MB, k1 = k0 + MB - 1;
+    finish_list<FAST, CAP>(sm, count, K, occ, lane, ws);
+    return count;
+}
+
+// The chunk list from the forward's record: the recorded leaves (at most the list capacity) get
+// the same exact leaf test as in a traversal, without the traversal.
+template <bool FAST, int CAP>
+__device__ int replay_list(WarpSmem<FAST, CAP>& sm, const RenderArgs& a, const RayState& r, bool on, float seg_hi,
+                           int K, int nv, const unsigned* ids, int n, int lane, WarpStats& ws) {
+    int count = 0;
+    unsigned long long occ[4] = {0ull, 0ull, 0ull, 0ull};
+    n = min(n, CAP);
+    for (int base = 0; base < n; base += 32) {
+        const int m = min(32, n - base);
+        const int mine = lane < m ? (int)ids[base + lane] : 0;
 #pragma unroll 1
-        for (int w = 0; w < nw; ++w) {
-            unsigned mw = 0u;
-            const int e0 = 32 * w, e1 = min(count, e0 + 32);
-#pragma unroll 1
-            for (int e = e0; e < e1; ++e) {
-                unsigned u = sm.urng[e];
-                if (k1 >= (int)(u & 0xffff) && k0 <= (int)(u >> 16)) mw |= 1u << (e - e0);
-            }
-            sm.smask[bk][w] = mw;
+        for (int j = 0; j < m; ++j) {
+            const int leaf = __shfl_sync(kFull, mine, j);
+            if (leaf >= 0 && leaf < a.n_leaves)
+                leaf_entry<FAST, CAP>(sm, a, r, on, seg_hi, K, nv, leaf, count, occ, lane, ws);
         }
     }
-    __syncwarp();
+    finish_list<FAST, CAP>(sm, count, K, occ, lane, ws);
     return count;
 }
 
@@ -428,18 +484,20 @@ __device__ __forceinline__ int slab_buffers(const WarpSmem<FAST, CAP>& sm, int k
                    r2 = f3(rec.r2.x, rec.r2.y, rec.r2.z);
             ++nh;
             if (FAST) {
+                // log2(dens * w_i) = log2(dens) - q_i log2(e) / 2, q_i quadratic in the sample index
                 float3 v0 = (r.o + r.d * r.tb) - mu;
                 float3 vb = r.d * kDt;
                 float3 m0 = f3(dot3(r0, v0), dot3(r1, v0), dot3(r2, v0));
                 float3 mb = f3(dot3(r0, vb), dot3(r1, vb), dot3(r2, vb));
-                float A = dot3(m0, m0), B2 = 2.f * dot3(m0, mb), Cq = dot3(mb, mb);
+                float A = fmaf(kNegHalfLog2e, dot3(m0, m0), lg2_approx(dn));
+                float B2 = (2.f * kNegHalfLog2e) * dot3(m0, mb), Cq = kNegHalfLog2e * dot3(mb, mb);
                 float3 col = f3(col4.x, col4.y, col4.z);
 #pragma unroll
                 for (int i = 0; i < kBuf; ++i) {
                     float fi = (float)i;
-                    float qv = fmaf(fi, fmaf(fi, Cq, B2), A);
-                    float dw = dn * ex2_approx(kNegHalfLog2e * qv);
-                    if (dw > kSigThr) {
+                    float e = fmaf(fi, fmaf(fi, Cq, B2), A);
+                    if (e > kLog2SigThr) {
+                        float dw = ex2_approx(e);
                         sig[i] += dw;
                         C[i] = C[i] + col * dw;
                     }
@@ -554,7 +612,7 @@ __device__ __forceinline__ float transpose_reduce16(float* v, int lane) {
 template <bool FAST, int CAP>
 __device__ __forceinline__ void slab_adjoint(const WarpSmem<FAST, CAP>& sm, int k, int K, bool has, const RayState& r,
                                              const RenderArgs& a, long long rgb_base, const float* roff,
-                                             const float* E, const float* F, const float* G, int nw, int lane,
+                                             const float* H, const float* F, int nw, int lane,
                                              WarpStats& ws) {
     const int vid = ((lane >> 4) & 1) * 8 + ((lane >> 3) & 1) * 4 + ((lane >> 2) & 1) * 2 + ((lane >> 1) & 1);
 #pragma unroll 1
@@ -595,22 +653,24 @@ __device__ __forceinline__ void slab_adjoint(const WarpSmem<FAST, CAP>& sm, int 
             const float3 mb = f3(dot3(r0, vb), dot3(r1, vb), dot3(r2, vb));
             float U0 = 0.f, U1 = 0.f, U2 = 0.f;
             if (FAST) {
-                float A = dot3(m0, m0), B2 = 2.f * dot3(m0, mb), Cq = dot3(mb, mb);
+                // dw_i = dens * w_i in the exponent domain (as in the forward); accumulates
+                // sum dw F, sum dw h and the moments of u = dw h, then divides by dens once
+                float A = fmaf(kNegHalfLog2e, dot3(m0, m0), lg2_approx(dn));
+                float B2 = (2.f * kNegHalfLog2e) * dot3(m0, mb), Cq = kNegHalfLog2e * dot3(mb, mb);
 #pragma unroll
                 for (int i = 0; i < kBuf; ++i) {
                     float fi = (float)i;
-                    float qv = fmaf(fi, fmaf(fi, Cq, B2), A);
-                    float wt = ex2_approx(kNegHalfLog2e * qv);
-                    if (dn * wt > kSigThr) {
-                        float h = E[i] + F[i] * (gcol - G[i]);
-                        gc += wt * F[i];
-                        dd += wt * h;
-                        float u = h * wt;
+                    float e = fmaf(fi, fmaf(fi, Cq, B2), A);
+                    if (e > kLog2SigThr) {
+                        float dw = ex2_approx(e);
+                        float u = fmaf(F[i], gcol, H[i]) * dw;
+                        gc = fmaf(dw, F[i], gc);
                         U0 += u;
-                        U1 += fi * u;
-                        U2 += fi * fi * u;
+                        U1 = fmaf(fi, u, U1);
+                        U2 = fmaf(fi * fi, u, U2);
                     }
                 }
+                dd = (U0 != 0.f) ? U0 * __fdividef(1.f, dn) : 0.f;
             } else {
 #pragma unroll
                 for (int i = 0; i < kBuf; ++i) {
@@ -619,7 +679,7 @@ __device__ __forceinline__ void slab_adjoint(const WarpSmem<FAST, CAP>& sm, int 
                     bool in;
                     float wt = parity_weight(r.o, r.d, t, mu, r0, r1, r2, dn, vv, m, in);
                     if (in) {
-                        float h = E[i] + F[i] * (gcol - G[i]);
+                        float h = fmaf(F[i], gcol, H[i]);
                         gc += wt * F[i];
                         dd += wt * h;
                         float u = h * wt;
@@ -629,10 +689,10 @@ __device__ __forceinline__ void slab_adjoint(const WarpSmem<FAST, CAP>& sm, int 
                         U2 += x * x * u;
                     }
                 }
-            }
-            {
                 gc *= dn;
                 U0 *= dn; U1 *= dn; U2 *= dn;
+            }
+            {
                 float3 Sm = m0 * U0 + mb * U1;
                 float3 Smm = f3(m0.x * m0.x * U0 + 2.f * m0.x * mb.x * U1 + mb.x * mb.x * U2,
                                 m0.y * m0.y * U0 + 2.f * m0.y * mb.y * U1 + mb.y * mb.y * U2,
@@ -677,11 +737,13 @@ __device__ __forceinline__ void slab_adjoint(const WarpSmem<FAST, CAP>& sm, int 
     }
 }
 
-// Per-sample compositing adjoint scalars of one slab (reference backward :675-730):
-// E = g.((T c - R) dt), F = T alpha / sigma, G = g.c ; advances T and R over the slab.
+// Per-sample compositing adjoint scalars of one slab (reference backward :675-730): with
+// E = g.((T c - R) dt), F = T alpha / sigma and G = g.c, a Gaussian of colour col and weight w
+// at the sample has dL/d(sigma-share) h = E + F (g.col - G) = F g.col + H, H = E - F G.
+// Returns H and F; advances T and R over the slab.
 template <bool FAST>
-__device__ __forceinline__ void slab_adjoint_scalars(const RayState& r, const float* sig, const float3* Cb, float* E,
-                                                     float* F, float* G, float& Ta, float3& Ra) {
+__device__ __forceinline__ void slab_adjoint_scalars(const RayState& r, const float* sig, const float3* Cb, float* H,
+                                                     float* F, float& Ta, float3& Ra) {
     Ta = r.T;
     Ra = r.C;
 #pragma unroll
@@ -695,9 +757,9 @@ __device__ __forceinline__ void slab_adjoint_scalars(const RayState& r, const fl
         }
         float alpha = FAST ? 1.f - exp_neg<true>(cd * kDt) : __fsub_rn(1.f, exp_neg<false>(__fmul_rn(cd, kDt)));
         float3 aux = (cc * Ta - Ra) * kDt;
-        E[i] = dot3(r.g, aux);
+        const float Ei = dot3(r.g, aux);
         F[i] = FAST ? Ta * alpha * inv : (cd > 0.f ? Ta * alpha / cd : 0.f);
-        G[i] = dot3(r.g, cc);
+        H[i] = Ei - F[i] * dot3(r.g, cc);
         Ra = Ra - cc * (Ta * alpha);
         Ta = FAST ? Ta * (1.f - alpha) : __fmul_rn(Ta, __fsub_rn(1.f, alpha));
     }
@@ -797,6 +859,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, min_blocks<BWD, FAST>()) 
             r.invd = f3(1.f / (fabsf(r.d.x) > tiny ? r.d.x : copysignf(tiny, r.d.x)),
                         1.f / (fabsf(r.d.y) > tiny ? r.d.y : copysignf(tiny, r.d.y)),
                         1.f / (fabsf(r.d.z) > tiny ? r.d.z : copysignf(tiny, r.d.z)));
+            r.oid = f3(-r.o.x * r.invd.x, -r.o.y * r.invd.y, -r.o.z * r.invd.z);
         }
         r.alive = valid && (r.tenter < r.texit);
         r.tb = r.tenter;
@@ -810,12 +873,30 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, min_blocks<BWD, FAST>()) 
 
         int K = min(kExactChunk, kmax);
         int rounds = 0;
+        // hit-list record of this tile: the forward appends chunk records, the backward replays them
+        const bool rec_here = a.rec_arena != nullptr && tile < a.rec_tiles;
+        if (lane == 0) {
+            sm.rec_first = kNoRecord;
+            sm.rec_prev = kNoRecord;
+            sm.rec_cur = (BWD && rec_here && a.replay) ? a.rec_tile[tile] : kNoRecord;
+        }
+        __syncwarp();
         while (true) {
             bool on = r.alive;
             if (!__any_sync(kFull, on)) break;
             if (++rounds > kMaxRounds) {
                 if (lane == 0) atomicAdd(&a.st->watchdog_trips, 1ull);
                 break;
+            }
+            unsigned rec_hdr = 0u;
+            unsigned rec_cur = BWD ? sm.rec_cur : kNoRecord;
+            if (BWD && rec_cur != kNoRecord) {
+                if (rec_cur + 2u > a.rec_cap) {
+                    rec_cur = kNoRecord;   // malformed link: traverse from here on
+                } else {
+                    rec_hdr = a.rec_arena[rec_cur];
+                    K = max(1, min(kmax, (int)((rec_hdr >> 16) & 0xffu)));
+                }
             }
             // slabs of this chunk: slab k is marched iff tb_k < texit (tb_k by repeated addition)
             int nv = 0;
@@ -834,13 +915,45 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, min_blocks<BWD, FAST>()) 
                 // a slab step that no longer changes tb (|t| beyond ~2^19) would march forever
                 if (!(r.tb < r.texit) || r.tb + kSlab == r.tb) { r.alive = false; on = false; nv = 0; }
             }
-            bool ovf;
-            int count = traverse<FAST, CAP>(sm, a, r, on, seg_hi, K, nv, -1, ovf, lane, ws);
+            bool ovf = false;
+            int count;
+            if (BWD && rec_cur != kNoRecord && !(rec_hdr & kRecordMulti)) {
+                const unsigned n_ids = min(rec_hdr & 0xffffu, a.rec_cap - rec_cur - 2u);
+                count = replay_list<FAST, CAP>(sm, a, r, on, seg_hi, K, nv, a.rec_arena + rec_cur + 2, (int)n_ids,
+                                               lane, ws);
+                ++ws.replays;
+            } else {
+                count = traverse<FAST, CAP>(sm, a, r, on, seg_hi, K, nv, -1, ovf, lane, ws);
+            }
             const unsigned long long* occ = sm.occ;
             if (ovf && K > 1) {
                 K = max(1, K >> 1);
                 if (lane == 0) atomicAdd(&a.st->chunk_splits, 1ull);
                 continue;
+            }
+            if (!BWD && rec_here && sm.rec_first != kRecordFailed) {
+                // chunk record: header (multi-pass flag | K << 16 | id count), next record, ids
+                const unsigned n_ids = ovf ? 0u : (unsigned)count;
+                const unsigned words = 2u + n_ids;
+                unsigned off = kNoRecord;
+                if (lane == 0) {
+                    unsigned long long o = atomicAdd(a.rec_top, (unsigned long long)words);
+                    if (o + words <= (unsigned long long)a.rec_cap) {
+                        off = (unsigned)o;
+                        a.rec_arena[off] = (ovf ? kRecordMulti : 0u) | ((unsigned)K << 16) | n_ids;
+                        a.rec_arena[off + 1] = kNoRecord;
+                        if (sm.rec_prev != kNoRecord) a.rec_arena[sm.rec_prev + 1] = off;
+                        if (sm.rec_first == kNoRecord) sm.rec_first = off;
+                        sm.rec_prev = off;
+                    } else {
+                        sm.rec_first = kRecordFailed;
+                        atomicAdd(&a.st->record_overflows, 1ull);
+                    }
+                }
+                off = __shfl_sync(kFull, off, 0);
+                if (off != kNoRecord)
+                    for (unsigned e = lane; e < n_ids; e += 32) a.rec_arena[off + 2 + e] = (unsigned)sm.ids[e];
+                __syncwarp();
             }
             if (!ovf) {
                 for (int k = 0; k < K; ++k) {
@@ -878,11 +991,11 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, min_blocks<BWD, FAST>()) 
                             r.seed = seed_next;
                         }
                     } else {
-                        float E[kBuf], F[kBuf], G[kBuf], Ta;
+                        float H[kBuf], F[kBuf], Ta;
                         float3 Ra;
-                        slab_adjoint_scalars<FAST>(r, sig, Cb, E, F, G, Ta, Ra);
+                        slab_adjoint_scalars<FAST>(r, sig, Cb, H, F, Ta, Ra);
                         bool act = has && nh > 0 && any_density(sig);
-                        slab_adjoint<FAST, CAP>(sm, k, K, act, r, a, rgb_base, roff, E, F, G, nwords(count), lane, ws);
+                        slab_adjoint<FAST, CAP>(sm, k, K, act, r, a, rgb_base, roff, H, F, nwords(count), lane, ws);
                         if (has && nh > 0) {
                             r.T = Ta;
                             r.C = Ra;
@@ -926,15 +1039,15 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, min_blocks<BWD, FAST>()) 
                         r.seed = seed_next;
                     }
                 } else {
-                    float E[kBuf], F[kBuf], G[kBuf], Ta;
+                    float H[kBuf], F[kBuf], Ta;
                     float3 Ra;
-                    slab_adjoint_scalars<FAST>(r, sig, Cb, E, F, G, Ta, Ra);
+                    slab_adjoint_scalars<FAST>(r, sig, Cb, H, F, Ta, Ra);
                     bool act = has && nh > 0 && any_density(sig);
                     int cursor = -1;
                     bool more2 = true;
                     while (more2) {
                         count = traverse<FAST, CAP>(sm, a, r, on, seg_hi, 1, nv, cursor, more2, lane, ws);
-                        slab_adjoint<FAST, CAP>(sm, 0, 1, act, r, a, rgb_base, roff, E, F, G, nwords(count), lane, ws);
+                        slab_adjoint<FAST, CAP>(sm, 0, 1, act, r, a, rgb_base, roff, H, F, nwords(count), lane, ws);
                         if (more2) cursor = sm.ids[count - 1];
                         __syncwarp();
                     }
@@ -947,7 +1060,11 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, min_blocks<BWD, FAST>()) 
                 if (has) r.tb = r.tb + kSlab;
             }
             if (on) r.alive = r.alive && (r.T > kTeps) && (r.tb < r.texit);
+            if (BWD && lane == 0) sm.rec_cur = (rec_cur != kNoRecord) ? a.rec_arena[rec_cur + 1] : kNoRecord;
+            __syncwarp();
         }
+        if (!BWD && rec_here && lane == 0)
+            a.rec_tile[tile] = (sm.rec_first == kRecordFailed) ? kNoRecord : sm.rec_first;
         if (!BWD && valid) {
             a.ray_colors[3 * ray_g] = __fadd_rn(r.C.x, __fmul_rn(r.T, bg));
             a.ray_colors[3 * ray_g + 1] = __fadd_rn(r.C.y, __fmul_rn(r.T, bg));
@@ -969,6 +1086,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, min_blocks<BWD, FAST>()) 
         atomicAdd(&a.st->list_entries, ws.entries);
         atomicAdd(&a.st->slab_steps, ws.slab_steps);
         atomicAdd(&a.st->entry_slabs, ws.entry_slabs);
+        if (BWD) atomicAdd(&a.st->replayed_chunks, ws.replays);
     }
 }
 

@@ -158,14 +158,16 @@ class Engine:
     def reserve(self, n, n_views=1, n_rays=0):
         check(self.lib.rg_reserve(self.h, int(n), int(n_views), int(n_rays)), self.h, "rg_reserve")
 
-    def set_tuning(self, chunk_slabs=0, blocks_per_sm=0, list_capacity=0):
-        t = _lib.rg_tuning(int(chunk_slabs), int(blocks_per_sm), int(list_capacity), 0)
+    def set_tuning(self, chunk_slabs=0, blocks_per_sm=0, list_capacity=0, record_hits=0):
+        """0 keeps a value; record_hits 1 / -1 switches the forward's hit-list record on / off."""
+        t = _lib.rg_tuning(int(chunk_slabs), int(blocks_per_sm), int(list_capacity), int(record_hits))
         check(self.lib.rg_set_tuning(self.h, ctypes.byref(t)), self.h, "rg_set_tuning")
 
     def get_tuning(self):
         t = _lib.rg_tuning()
         check(self.lib.rg_get_tuning(self.h, ctypes.byref(t)), self.h, "rg_get_tuning")
-        return dict(chunk_slabs=t.chunk_slabs, blocks_per_sm=t.blocks_per_sm, list_capacity=t.list_capacity)
+        return dict(chunk_slabs=t.chunk_slabs, blocks_per_sm=t.blocks_per_sm, list_capacity=t.list_capacity,
+                    record_hits=t.record_hits)
 
     def status(self, reset=False):
         st = _lib.rg_status()
@@ -241,6 +243,7 @@ class Engine:
         """RenderOptixFunction.forward: bbox -> BVH build (or refit) -> colour -> forward launch."""
         ray_colors = torch.empty((n_rays, 3), dtype=torch.float32, device=self.device)
         fT = torch.empty((n_rays,), dtype=torch.float32, device=self.device) if final_T else None
+        self.reserve(0, 0, n_rays)   # sizes the hit-list record once per ray count (no-op afterwards)
         with self._timed("prepare"):
             self.ellipsoids_bbox(g)
             if refit and self._built_n == g.n:
