@@ -87,6 +87,26 @@ def max_over_ranks(value: float, device) -> float:
     return float(t.item())
 
 
+def _profile_figures(name):
+    """key = value figures of a committed ncu summary under profiles/ (empty when absent)."""
+    out = {}
+    try:
+        with open(os.path.join(ROOT, "profiles", name)) as f:
+            for line in f:
+                if "=" in line and not line.lstrip().startswith("#"):
+                    k, v = line.split("=", 1)
+                    try:
+                        out[k.strip()] = float(v.split()[0])
+                    except (ValueError, IndexError):
+                        pass
+    except OSError:
+        pass
+    return out
+
+
+TRAFFIC_PROFILE = "k_render_traffic_unbounded_1m_16view.txt"
+
+
 def _peaks():
     try:
         with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
@@ -228,13 +248,23 @@ def our_arm(args, rank, world, local):
     # algorithmic bytes of one backward launch: leaf records (64 B) + scale/quaternion (32 B) + colour per
     # view (16 B) read once per Gaussian, gradient accumulators written once (48 B + 16 B per view), ray
     # colour and dL/dcolour read once per ray (24 B)
-    alg_bwd = n * (64 + 32 + 16 * V) + n * (48 + 16 * V) + 24 * R
+    # plus the forward's hit-list record, read once (4 B per recorded word)
+    rec_bytes = 4 * st.get("record_words", 0) // max(1, args.steps)
+    alg_bwd = n * (64 + 32 + 16 * V) + n * (48 + 16 * V) + 24 * R + rec_bytes
     peak, peak_kind = _peaks()
     achieved = alg_bwd / (bwd_ms * 1e-3) / 1e9
+    # DRAM traffic and SM issue utilisation of this launch from the committed ncu summary of the same
+    # workload (a profiler number is never timed here)
+    prof = _profile_figures(TRAFFIC_PROFILE)
+    traffic = None
+    if prof.get("gaussians") == n and prof.get("views") == V and "backward_dram_bytes" in prof:
+        traffic = int(prof["backward_dram_bytes"])
     roofline = {"bound": "hbm", "achieved": round(achieved, 2), "peak": peak, "unit": "GB/s",
-                "frac": round(achieved / peak, 5), "traffic": None, "peak_source": peak_kind,
+                "frac": round(achieved / peak, 5), "traffic": traffic, "peak_source": peak_kind,
                 "kernel": "k_render<backward> (rg_launch_backward)",
-                "algorithmic_bytes_per_launch": int(alg_bwd)}
+                "algorithmic_bytes_per_launch": int(alg_bwd),
+                "sm_issue_frac_ncu": prof.get("backward_sm_issue_frac"),
+                "note": "L2-resident gather/accumulate: bound by SM instruction issue, not HBM"}
     # step-level algorithmic bytes (parameters read twice, gradients written once, 36 B per ray)
     p_store = bytes_per_gaussian(nsg, ncoef, True)
     g_bytes = bytes_per_gaussian(nsg, ncoef, False)
