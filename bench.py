@@ -249,7 +249,7 @@ def our_arm(args, rank, world, local):
     # view (16 B) read once per Gaussian, gradient accumulators written once (48 B + 16 B per view), ray
     # colour and dL/dcolour read once per ray (24 B)
     # plus the forward's hit-list record, read once (4 B per recorded word)
-    rec_bytes = 4 * st.get("record_words", 0) // max(1, args.steps)
+    rec_bytes = 4 * st.get("record_words", 0)   # size of the last forward's record (not a running sum)
     alg_bwd = n * (64 + 32 + 16 * V) + n * (48 + 16 * V) + 24 * R + rec_bytes
     peak, peak_kind = _peaks()
     achieved = alg_bwd / (bwd_ms * 1e-3) / 1e9
@@ -389,7 +389,7 @@ def our_arm(args, rank, world, local):
                           "frac": round(b_step / (ms_max * 1e-3) / 1e9 / peak, 5)},
         "stage_ms": {"prepare(bbox+bvh+colour)": round(prep_ms, 3), "forward": round(fwd_ms, 3),
                      "backward": round(bwd_ms, 3), "backward_sh": round(shb_ms, 3)},
-        "counters_per_step": {k: v // max(1, args.steps) for k, v in st.items()},
+        "counters_per_step": {k: (v if k == "record_words" else v // max(1, args.steps)) for k, v in st.items()},
         "tuning": {k: v for k, v in tuning.items() if k != "ms"},
         "graph_replay": graph,
         "plain_fp32_single_view": plain,
