@@ -45,6 +45,7 @@ constexpr float kNegHalfLog2e = -0.72134752044448170f;
 constexpr float kLog2SigThr = -3.3219280948873623f;   // log2(0.1): per-sample density threshold
 constexpr float kInvSlab = 50.0f;          // 1 / 0.02
 constexpr int kExactChunk = 8;             // chunks up to this length use exact slab ranges
+constexpr int kCounters = 9;               // per-warp counters: the WarpStats fields, hit pairs, slabs
 constexpr unsigned kNoRecord = 0xffffffffu;     // hit-list record: no (next) chunk record
 constexpr unsigned kRecordMulti = 0x80000000u;  // chunk consumed in several traversal passes
 constexpr unsigned kRecordFailed = 0xfffffffeu; // the tile's record did not fit the arena
@@ -70,12 +71,14 @@ struct WarpSmem {
     // hit-list record of the warp's current tile (written by lane 0)
     unsigned rec_first, rec_prev;                    // forward: first / last chunk record
     unsigned rec_cur;                                // backward: next chunk record to replay
+    unsigned long long cnt[kCounters];               // activity counters of the warp (lane 0)
 };
 
-// Warp-uniform activity counters (flushed once per warp).
+// Warp-uniform activity counters of one tile (32-bit; added to the warp's shared-memory totals at
+// the end of the tile so that few registers stay live through the traversal and slab loops).
 struct WarpStats {
-    unsigned long long traversals = 0, node_visits = 0, leaf_tests = 0, entries = 0, slab_steps = 0,
-                       entry_slabs = 0, replays = 0;
+    unsigned traversals = 0, node_visits = 0, leaf_tests = 0, entries = 0, slab_steps = 0, entry_slabs = 0,
+             replays = 0;
 };
 
 struct RayState {
@@ -249,13 +252,44 @@ __device__ __forceinline__ int occ_next(const unsigned long long* occ, int k, in
     return K;
 }
 
+template <bool FAST, int CAP>
+__device__ __forceinline__ void clear_occ(WarpSmem<FAST, CAP>& sm, int lane) {
+    if (lane == 0) {
+#pragma unroll
+        for (int w = 0; w < 4; ++w) sm.occ[w] = 0ull;
+    }
+}
+
+// Adds the tile's counters to the warp's totals and resets them.
+template <bool FAST, int CAP>
+__device__ __forceinline__ void flush_stats(WarpSmem<FAST, CAP>& sm, WarpStats& ws, unsigned hits, unsigned slabs,
+                                            int lane) {
+#pragma unroll
+    for (int o = 16; o; o >>= 1) {
+        hits += __shfl_xor_sync(kFull, hits, o);
+        slabs += __shfl_xor_sync(kFull, slabs, o);
+    }
+    if (lane == 0) {
+        sm.cnt[0] += ws.traversals;
+        sm.cnt[1] += ws.node_visits;
+        sm.cnt[2] += ws.leaf_tests;
+        sm.cnt[3] += ws.entries;
+        sm.cnt[4] += ws.slab_steps;
+        sm.cnt[5] += ws.entry_slabs;
+        sm.cnt[6] += ws.replays;
+        sm.cnt[7] += hits;
+        sm.cnt[8] += slabs;
+    }
+    ws = WarpStats();
+}
+
 // Exact leaf test of every active lane for the chunk [tb, seg_hi]: appends the leaf to the warp
 // list when any lane's interval meets one of the chunk's slabs.  Returns false (leaf not taken)
 // when the list is already full.
 template <bool FAST, int CAP>
 __device__ __forceinline__ bool leaf_entry(WarpSmem<FAST, CAP>& sm, const RenderArgs& a, const RayState& r, bool on,
-                                           float seg_hi, int K, int nv, int leaf, int& count,
-                                           unsigned long long* occ, int lane, WarpStats& ws) {
+                                           float seg_hi, int K, int nv, int leaf, int& count, int lane,
+                                           WarpStats& ws) {
     ++ws.leaf_tests;
     int lo = 255, hi = -1;
     if (on) {
@@ -282,21 +316,16 @@ __device__ __forceinline__ bool leaf_entry(WarpSmem<FAST, CAP>& sm, const Render
     if (lane == 0) {
         sm.ids[count] = leaf;
         sm.urng[count] = (unsigned)ulo | ((unsigned)uhi << 16);
+        occ_set(sm.occ, ulo, uhi);
     }
-    occ_set(occ, ulo, uhi);
     ++count;
     return true;
 }
 
 // Publishes the chunk list: occupancy bits and the entry masks per block of MB slabs.
 template <bool FAST, int CAP>
-__device__ __forceinline__ void finish_list(WarpSmem<FAST, CAP>& sm, int count, int K, const unsigned long long* occ,
-                                            int lane, WarpStats& ws) {
+__device__ __forceinline__ void finish_list(WarpSmem<FAST, CAP>& sm, int count, int K, int lane, WarpStats& ws) {
     __syncwarp();
-    if (lane == 0) {
-#pragma unroll
-        for (int w = 0; w < 4; ++w) sm.occ[w] = occ[w];
-    }
     ws.entries += count;
     // lane l fills blocks l, l+32
     constexpr int MB = WarpSmem<FAST, CAP>::MB;
@@ -328,7 +357,7 @@ __device__ int traverse(WarpSmem<FAST, CAP>& sm, const RenderArgs& a, const RayS
     int count = 0;
     ++ws.traversals;
     ovf = false;
-    unsigned long long occ[4] = {0ull, 0ull, 0ull, 0ull};
+    clear_occ(sm, lane);
     int sp = 0;
     int cur = (a.n_leaves == 1) ? ~0 : 0;
     long long guard = 0;
@@ -363,7 +392,7 @@ __device__ int traverse(WarpSmem<FAST, CAP>& sm, const RenderArgs& a, const RayS
             if (br) { cur = n3.y; continue; }
         } else {
             int leaf = ~cur;
-            if (leaf > cursor && !leaf_entry<FAST, CAP>(sm, a, r, on, seg_hi, K, nv, leaf, count, occ, lane, ws)) {
+            if (leaf > cursor && !leaf_entry<FAST, CAP>(sm, a, r, on, seg_hi, K, nv, leaf, count, lane, ws)) {
                 ovf = true;
                 break;
             }
@@ -372,7 +401,7 @@ __device__ int traverse(WarpSmem<FAST, CAP>& sm, const RenderArgs& a, const RayS
         __syncwarp();
         cur = sm.stack[--sp];
     }
-    finish_list<FAST, CAP>(sm, count, K, occ, lane, ws);
+    finish_list<FAST, CAP>(sm, count, K, lane, ws);
     return count;
 }
 
@@ -382,7 +411,7 @@ template <bool FAST, int CAP>
 __device__ int replay_list(WarpSmem<FAST, CAP>& sm, const RenderArgs& a, const RayState& r, bool on, float seg_hi,
                            int K, int nv, const unsigned* ids, int n, int lane, WarpStats& ws) {
     int count = 0;
-    unsigned long long occ[4] = {0ull, 0ull, 0ull, 0ull};
+    clear_occ(sm, lane);
     n = min(n, CAP);
     for (int base = 0; base < n; base += 32) {
         const int m = min(32, n - base);
@@ -391,10 +420,10 @@ __device__ int replay_list(WarpSmem<FAST, CAP>& sm, const RenderArgs& a, const R
         for (int j = 0; j < m; ++j) {
             const int leaf = __shfl_sync(kFull, mine, j);
             if (leaf >= 0 && leaf < a.n_leaves)
-                leaf_entry<FAST, CAP>(sm, a, r, on, seg_hi, K, nv, leaf, count, occ, lane, ws);
+                leaf_entry<FAST, CAP>(sm, a, r, on, seg_hi, K, nv, leaf, count, lane, ws);
         }
     }
-    finish_list<FAST, CAP>(sm, count, K, occ, lane, ws);
+    finish_list<FAST, CAP>(sm, count, K, lane, ws);
     return count;
 }
 
@@ -796,8 +825,10 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, min_blocks<BWD, FAST>()) 
     float scene[6];
 #pragma unroll
     for (int z = 0; z < 6; ++z) scene[z] = ord2f(a.scene_ord[z]);
-    unsigned long long hits_acc = 0, slabs_acc = 0;
-    WarpStats ws;
+    if (lane == 0) {
+#pragma unroll
+        for (int c = 0; c < kCounters; ++c) sm.cnt[c] = 0ull;
+    }
     const int kmax =
         min((a.rnd_sample == 1) ? min(a.chunk_slabs, kExactChunk) : a.chunk_slabs, WarpSmem<FAST, CAP>::KM);
 
@@ -825,6 +856,8 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, min_blocks<BWD, FAST>()) 
         const long long rgb_base = (long long)view * a.n_leaves;
 
         RayState r;
+        WarpStats ws;
+        unsigned hits_acc = 0, slabs_acc = 0;   // this lane's (slab, Gaussian) pairs and slabs
         r.seed = tea4(a.iteration, ray_l);
         {
             // computeRay (forward/gaussians_aabb.cu:405-434) in IEEE operation order
@@ -1065,6 +1098,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, min_blocks<BWD, FAST>()) 
         }
         if (!BWD && rec_here && lane == 0)
             a.rec_tile[tile] = (sm.rec_first == kRecordFailed) ? kNoRecord : sm.rec_first;
+        flush_stats(sm, ws, hits_acc, slabs_acc, lane);
         if (!BWD && valid) {
             a.ray_colors[3 * ray_g] = __fadd_rn(r.C.x, __fmul_rn(r.T, bg));
             a.ray_colors[3 * ray_g + 1] = __fadd_rn(r.C.y, __fmul_rn(r.T, bg));
@@ -1072,21 +1106,18 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, min_blocks<BWD, FAST>()) 
             if (a.final_T) a.final_T[ray_g] = r.T;
         }
     }
-    // counters: warp reduction, one atomic per warp
-    for (int o = 16; o; o >>= 1) {
-        hits_acc += __shfl_xor_sync(kFull, hits_acc, o);
-        slabs_acc += __shfl_xor_sync(kFull, slabs_acc, o);
-    }
+    // counters: one atomic per warp and counter
+    __syncwarp();
     if (lane == 0) {
-        atomicAdd(&a.st->hit_pairs, hits_acc);
-        atomicAdd(&a.st->slabs, slabs_acc);
-        atomicAdd(&a.st->traversals, ws.traversals);
-        atomicAdd(&a.st->node_visits, ws.node_visits);
-        atomicAdd(&a.st->leaf_tests, ws.leaf_tests);
-        atomicAdd(&a.st->list_entries, ws.entries);
-        atomicAdd(&a.st->slab_steps, ws.slab_steps);
-        atomicAdd(&a.st->entry_slabs, ws.entry_slabs);
-        if (BWD) atomicAdd(&a.st->replayed_chunks, ws.replays);
+        atomicAdd(&a.st->traversals, sm.cnt[0]);
+        atomicAdd(&a.st->node_visits, sm.cnt[1]);
+        atomicAdd(&a.st->leaf_tests, sm.cnt[2]);
+        atomicAdd(&a.st->list_entries, sm.cnt[3]);
+        atomicAdd(&a.st->slab_steps, sm.cnt[4]);
+        atomicAdd(&a.st->entry_slabs, sm.cnt[5]);
+        if (BWD) atomicAdd(&a.st->replayed_chunks, sm.cnt[6]);
+        atomicAdd(&a.st->hit_pairs, sm.cnt[7]);
+        atomicAdd(&a.st->slabs, sm.cnt[8]);
     }
 }
 
