@@ -175,7 +175,7 @@ RG_API int rg_bvh_build(rg_engine* e, void* stream);
 RG_API int rg_bvh_refit(rg_engine* e, void* stream);
 
 /* utils/sh_utils.cu:25-119 for n_cams views at once.  cams is a DEVICE array of rg_camera.
- * rgb_out (n_cams,N,3) is an optional device output in Gaussian order. */
+ * rgb_out (n_cams,N,3) is an optional device output in Gaussian order.  n_cams * N < 2^31. */
 RG_API int rg_forward_sh(rg_engine* e, const rg_gaussians* g, const rg_camera* cams, int32_t n_cams,
                   float* rgb_out, void* stream);
 

@@ -155,6 +155,11 @@ int check_views(const rg_camera* cams, int n_cams) {
     return RG_OK;
 }
 
+// The per-(view, leaf) colour and gradient tables are indexed with 32-bit offsets.
+int check_table(long long n, int n_cams) {
+    return (long long)n_cams * n >= (long long)INT_MAX ? RG_ERR_INVALID_ARG : RG_OK;
+}
+
 cudaStream_t S(void* s) { return reinterpret_cast<cudaStream_t>(s); }
 
 int set_device(rg_engine* e) {
@@ -339,6 +344,7 @@ int rg_forward_sh(rg_engine* e, const rg_gaussians* g, const rg_camera* cams, in
     int rc = check_gaussians(g);
     if (rc || (rc = check_views(cams, n_cams))) return rc;
     if (e->n_built != g->n) return RG_ERR_STATE;
+    if ((rc = check_table(g->n, n_cams))) return rc;
     if ((rc = set_device(e)) || (rc = ensure_views(e, n_cams))) return rc;
     RG_CUDA(rg::launch_color_forward(g, cams, n_cams, e->bvh.rank, e->rgb_leaf, rgb_out, S(stream)), "forward_sh");
     e->launches += 1;

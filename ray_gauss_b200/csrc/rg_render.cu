@@ -491,7 +491,7 @@ __device__ __forceinline__ bool lane_has_entry(const WarpSmem<FAST, CAP>& sm, co
 // Sample buffers of slab k: sum of density and density-weighted colour of the lane's hits.
 template <bool FAST, int CAP>
 __device__ __forceinline__ int slab_buffers(const WarpSmem<FAST, CAP>& sm, int k, int K, bool has, const RayState& r,
-                                            const RenderArgs& a, long long rgb_base, const float* roff,
+                                            const RenderArgs& a, int rgb_base, const float* roff,
                                             float* sig, float3* C, int nw, int lane, WarpStats& ws) {
     int nh = 0;
 #pragma unroll 1
@@ -640,7 +640,7 @@ __device__ __forceinline__ float transpose_reduce16(float* v, int lane) {
 // one atomic per value.  Value order: ddens, dpos.xyz, dscale.xyz, dquat.xyzw, drgb.xyz.
 template <bool FAST, int CAP>
 __device__ __forceinline__ void slab_adjoint(const WarpSmem<FAST, CAP>& sm, int k, int K, bool has, const RayState& r,
-                                             const RenderArgs& a, long long rgb_base, const float* roff,
+                                             const RenderArgs& a, int rgb_base, const float* roff,
                                              const float* H, const float* F, int nw, int lane,
                                              WarpStats& ws) {
     const int vid = ((lane >> 4) & 1) * 8 + ((lane >> 3) & 1) * 4 + ((lane >> 2) & 1) * 2 + ((lane >> 1) & 1);
@@ -822,9 +822,6 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, min_blocks<BWD, FAST>()) 
     WarpSmem<FAST, CAP>& sm = smem[threadIdx.x >> 5];
     const ViewTable* vt = a.views;
     const float bg = a.white_bg ? 1.f : 0.f;
-    float scene[6];
-#pragma unroll
-    for (int z = 0; z < 6; ++z) scene[z] = ord2f(a.scene_ord[z]);
     if (lane == 0) {
 #pragma unroll
         for (int c = 0; c < kCounters; ++c) sm.cnt[c] = 0ull;
@@ -852,8 +849,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, min_blocks<BWD, FAST>()) 
         const int py = (local / tiles_x) * kTileH + (lane / kTileW);
         const bool valid = px < W && py < H;
         const unsigned ray_l = (unsigned)(py * W + px);
-        const long long ray_g = vt->ray_prefix[view] + (long long)ray_l;
-        const long long rgb_base = (long long)view * a.n_leaves;
+        const int rgb_base = view * a.n_leaves;   // views x leaves < 2^31 (checked by the host)
 
         RayState r;
         WarpStats ws;
@@ -881,6 +877,9 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, min_blocks<BWD, FAST>()) 
             r.o = f3(cam.eye[0], cam.eye[1], cam.eye[2]);
         }
         {
+            float scene[6];   // scene box, read per tile (not kept live through the tile's loops)
+#pragma unroll
+            for (int z = 0; z < 6; ++z) scene[z] = ord2f(__ldg(a.scene_ord + z));
             float t0x = __fdiv_rn(scene[0] - r.o.x, r.d.x), t1x = __fdiv_rn(scene[3] - r.o.x, r.d.x);
             float t0y = __fdiv_rn(scene[1] - r.o.y, r.d.y), t1y = __fdiv_rn(scene[4] - r.o.y, r.d.y);
             float t0z = __fdiv_rn(scene[2] - r.o.z, r.d.z), t1z = __fdiv_rn(scene[5] - r.o.z, r.d.z);
@@ -900,6 +899,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, min_blocks<BWD, FAST>()) 
         r.C = f3(0.f, 0.f, 0.f);
         r.g = f3(0.f, 0.f, 0.f);
         if (BWD && valid) {
+            const long long ray_g = vt->ray_prefix[view] + (long long)ray_l;
             r.C = f3(a.ray_colors_in[3 * ray_g], a.ray_colors_in[3 * ray_g + 1], a.ray_colors_in[3 * ray_g + 2]);
             r.g = f3(a.dL[3 * ray_g], a.dL[3 * ray_g + 1], a.dL[3 * ray_g + 2]);
         }
@@ -1100,6 +1100,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, min_blocks<BWD, FAST>()) 
             a.rec_tile[tile] = (sm.rec_first == kRecordFailed) ? kNoRecord : sm.rec_first;
         flush_stats(sm, ws, hits_acc, slabs_acc, lane);
         if (!BWD && valid) {
+            const long long ray_g = vt->ray_prefix[view] + (long long)ray_l;
             a.ray_colors[3 * ray_g] = __fadd_rn(r.C.x, __fmul_rn(r.T, bg));
             a.ray_colors[3 * ray_g + 1] = __fadd_rn(r.C.y, __fmul_rn(r.T, bg));
             a.ray_colors[3 * ray_g + 2] = __fadd_rn(r.C.z, __fmul_rn(r.T, bg));
