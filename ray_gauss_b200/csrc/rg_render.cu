@@ -360,35 +360,38 @@ __device__ int traverse(WarpSmem<FAST, CAP>& sm, const RenderArgs& a, const RayS
     clear_occ(sm, lane);
     int sp = 0;
     int cur = (a.n_leaves == 1) ? ~0 : 0;
-    long long guard = 0;
-    const long long guard_max = 4ll * a.n_leaves + 64;
+    unsigned guard = 0, visits = 0;
+    const unsigned guard_max = 4u * (unsigned)a.n_leaves + 64u;
     while (true) {
         if (++guard > guard_max) {
             if (lane == 0) atomicAdd(&a.st->watchdog_trips, 1ull);
             break;
         }
         if (cur >= 0) {
-            ++ws.node_visits;
+            ++visits;
             const float4* np = reinterpret_cast<const float4*>(a.nodes + cur);
             float4 n0 = __ldg(np), n1 = __ldg(np + 1), n2 = __ldg(np + 2);
             int4 n3 = __ldg(reinterpret_cast<const int4*>(np + 3));
             float lb[6] = {n0.x, n0.y, n0.z, n0.w, n1.x, n1.y};
             float rb[6] = {n1.z, n1.w, n2.x, n2.y, n2.z, n2.w};
-            bool hl = on && n3.z > cursor && box_hit<FAST>(lb, r, r.tb, seg_hi);
-            bool hr = on && n3.w > cursor && box_hit<FAST>(rb, r, r.tb, seg_hi);
-            unsigned bl = __ballot_sync(kFull, hl), br = __ballot_sync(kFull, hr);
-            if (bl && br) {
-                if (sp < kStack) {
-                    if (lane == 0) sm.stack[sp] = n3.y;
-                    ++sp;
-                } else if (lane == 0) {
-                    atomicAdd(&a.st->stack_overflows, 1ull);
+            // non-short-circuit predicates: no branches before the ballots
+            const bool hl = box_hit<FAST>(lb, r, r.tb, seg_hi) & on & (n3.z > cursor);
+            const bool hr = box_hit<FAST>(rb, r, r.tb, seg_hi) & on & (n3.w > cursor);
+            const unsigned bl = __ballot_sync(kFull, hl), br = __ballot_sync(kFull, hr);
+            if (bl) {
+                if (br) {
+                    // every lane stores the same value and reads back only its own stores: the
+                    // stack needs neither a single writer nor a warp barrier
+                    if (sp < kStack) {
+                        sm.stack[sp] = n3.y;
+                        ++sp;
+                    } else if (lane == 0) {
+                        atomicAdd(&a.st->stack_overflows, 1ull);
+                    }
                 }
-                __syncwarp();
                 cur = n3.x;
                 continue;
             }
-            if (bl) { cur = n3.x; continue; }
             if (br) { cur = n3.y; continue; }
         } else {
             int leaf = ~cur;
@@ -398,9 +401,9 @@ __device__ int traverse(WarpSmem<FAST, CAP>& sm, const RenderArgs& a, const RayS
             }
         }
         if (sp == 0) break;
-        __syncwarp();
         cur = sm.stack[--sp];
     }
+    ws.node_visits += visits;
     finish_list<FAST, CAP>(sm, count, K, lane, ws);
     return count;
 }
