@@ -85,6 +85,17 @@ __device__ __forceinline__ float ex2_approx(float x) {
     asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
     return y;
 }
+// Three-input min / max (one instruction on sm_100)
+__device__ __forceinline__ float max3f(float a, float b, float c) {
+    float d;
+    asm("max.f32 %0, %1, %2, %3;" : "=f"(d) : "f"(a), "f"(b), "f"(c));
+    return d;
+}
+__device__ __forceinline__ float min3f(float a, float b, float c) {
+    float d;
+    asm("min.f32 %0, %1, %2, %3;" : "=f"(d) : "f"(a), "f"(b), "f"(c));
+    return d;
+}
 // SFU base-2 logarithm (x <= 0 gives -inf / NaN, which fail every threshold comparison)
 __device__ __forceinline__ float lg2_approx(float x) {
     float y;
@@ -130,7 +141,7 @@ struct __align__(16) GaussRec {
 
 // BVH internal node, 64 bytes: child boxes, child ids (>= 0 internal, < 0 leaf ~id),
 // split position and last leaf of the node's range.
-struct __align__(16) Node {
+struct __align__(32) Node {   // 32-byte aligned for 256-bit loads
     float4 n0;  // lbox lo.xyz, lbox hi.x
     float4 n1;  // lbox hi.yz, rbox lo.xy
     float4 n2;  // rbox lo.z, rbox hi.xyz

@@ -116,9 +116,26 @@ __device__ __forceinline__ bool box_hit(const float* bx, const RayState& r, floa
         ty0 = (bx[1] - r.o.y) * r.invd.y; ty1 = (bx[4] - r.o.y) * r.invd.y;
         tz0 = (bx[2] - r.o.z) * r.invd.z; tz1 = (bx[5] - r.o.z) * r.invd.z;
     }
-    float tn = fmaxf(fmaxf(lo, fminf(tx0, tx1)), fmaxf(fminf(ty0, ty1), fminf(tz0, tz1)));
-    float tf = fminf(fminf(hi, fmaxf(tx0, tx1)), fminf(fmaxf(ty0, ty1), fmaxf(tz0, tz1)));
+    float tn = fmaxf(max3f(fminf(tx0, tx1), fminf(ty0, ty1), fminf(tz0, tz1)), lo);
+    float tf = fminf(min3f(fmaxf(tx0, tx1), fmaxf(ty0, ty1), fmaxf(tz0, tz1)), hi);
     return tn <= tf;
+}
+
+// A 64-byte node in two 256-bit read-only loads (nodes are 64-byte aligned).
+__device__ __forceinline__ void load_node(const Node* p, float (&lb)[6], float (&rb)[6], int4& n3) {
+    float f[8];
+    unsigned u[8];
+    asm("ld.global.nc.v8.f32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
+        : "=f"(f[0]), "=f"(f[1]), "=f"(f[2]), "=f"(f[3]), "=f"(f[4]), "=f"(f[5]), "=f"(f[6]), "=f"(f[7])
+        : "l"(p));
+    asm("ld.global.nc.v8.b32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
+        : "=r"(u[0]), "=r"(u[1]), "=r"(u[2]), "=r"(u[3]), "=r"(u[4]), "=r"(u[5]), "=r"(u[6]), "=r"(u[7])
+        : "l"(reinterpret_cast<const char*>(p) + 32));
+    lb[0] = f[0]; lb[1] = f[1]; lb[2] = f[2]; lb[3] = f[3]; lb[4] = f[4]; lb[5] = f[5];
+    rb[0] = f[6]; rb[1] = f[7];
+    rb[2] = __uint_as_float(u[0]); rb[3] = __uint_as_float(u[1]); rb[4] = __uint_as_float(u[2]);
+    rb[5] = __uint_as_float(u[3]);
+    n3 = make_int4((int)u[4], (int)u[5], (int)u[6], (int)u[7]);
 }
 
 __device__ __forceinline__ LeafRec load_rec(const LeafRec* p, int i) {
@@ -369,11 +386,9 @@ __device__ int traverse(WarpSmem<FAST, CAP>& sm, const RenderArgs& a, const RayS
         }
         if (cur >= 0) {
             ++visits;
-            const float4* np = reinterpret_cast<const float4*>(a.nodes + cur);
-            float4 n0 = __ldg(np), n1 = __ldg(np + 1), n2 = __ldg(np + 2);
-            int4 n3 = __ldg(reinterpret_cast<const int4*>(np + 3));
-            float lb[6] = {n0.x, n0.y, n0.z, n0.w, n1.x, n1.y};
-            float rb[6] = {n1.z, n1.w, n2.x, n2.y, n2.z, n2.w};
+            float lb[6], rb[6];
+            int4 n3;
+            load_node(a.nodes + cur, lb, rb, n3);
             // non-short-circuit predicates: no branches before the ballots
             const bool hl = box_hit<FAST>(lb, r, r.tb, seg_hi) & on & (n3.z > cursor);
             const bool hr = box_hit<FAST>(rb, r, r.tb, seg_hi) & on & (n3.w > cursor);
