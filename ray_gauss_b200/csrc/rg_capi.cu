@@ -417,7 +417,8 @@ int rg_launch_backward(rg_engine* e, const rg_camera* cams, int32_t n_cams, cons
     }
     int grid = render_grid(e, true, s->mode);
     RG_CUDA(rg::launch_render(true, s->mode, e->tuning.list_capacity, grid, a, S(stream)), "render backward");
-    e->launches += 2;
+    RG_CUDA(rg::launch_moment_grads((int)N, e->bvh.leaf_rec, e->bvh.leaf_ext, e->gacc_geo, S(stream)), "moments");
+    e->launches += 3;
     return RG_OK;
 }
 

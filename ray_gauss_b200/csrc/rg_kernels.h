@@ -44,7 +44,8 @@ struct RenderArgs {
     // backward inputs / outputs
     const float* ray_colors_in;
     const float* dL;
-    float4* gacc_geo;             // (n_leaves, 3): ddens, dpos.xyz, dscale.xyz, dquat.xyzw, pad
+    float4* gacc_geo;             // (n_leaves, 3): ddens, dpos.xyz, dscale.xyz, dquat.xyzw, pad (the
+                                  // render kernel accumulates moments there; launch_moment_grads converts)
     float4* gacc_rgb;             // (n_views, n_leaves): {drgb.xyz, 0}
     int* work_counter;
     DevStatus* st;
@@ -67,6 +68,7 @@ cudaError_t launch_build(long long n, const float* aabb, const int* scene_ord, c
 cudaError_t launch_refit(long long n, const float* aabb, const GaussRec* rec, const rg_gaussians* g,
                          BvhBuffers& b, cudaStream_t s);
 
+cudaError_t launch_moment_grads(int n, const LeafRec* rec, const float4* ext, float4* acc, cudaStream_t s);
 cudaError_t launch_setup_views(const rg_camera* cams, int n_cams, ViewTable* vt, int* work_counter,
                                cudaStream_t s);
 cudaError_t launch_color_forward(const rg_gaussians* g, const rg_camera* cams, int n_cams, const int* rank,

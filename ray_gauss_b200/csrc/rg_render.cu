@@ -655,7 +655,7 @@ __device__ __forceinline__ float transpose_reduce16(float* v, int lane) {
 }
 
 // Adjoint of slab k for all list entries: per-lane gradient of each hit Gaussian, warp reduction,
-// one atomic per value.  Value order: ddens, dpos.xyz, dscale.xyz, dquat.xyzw, drgb.xyz.
+// one atomic per value.  Value order: ddens, S1.xyz, M2 (xx yy zz xy xz yz), 0, drgb.xyz.
 template <bool FAST, int CAP>
 __device__ __forceinline__ void slab_adjoint(const WarpSmem<FAST, CAP>& sm, int k, int K, bool has, const RayState& r,
                                              const RenderArgs& a, int rgb_base, const float* roff,
@@ -680,28 +680,28 @@ __device__ __forceinline__ void slab_adjoint(const WarpSmem<FAST, CAP>& sm, int 
         if (act) {
             LeafRec rec = load_rec(a.rec, leaf);
             float4 col4 = __ldg(a.rgb + rgb_base + leaf);
-            float4 s4 = __ldg(a.ext + 2 * (long long)leaf);
-            float4 q4 = __ldg(a.ext + 2 * (long long)leaf + 1);
             float3 mu = f3(rec.a.x, rec.a.y, rec.a.z);
             float dn = rec.a.w;
             float3 r0 = f3(rec.r0.x, rec.r0.y, rec.r0.z), r1 = f3(rec.r1.x, rec.r1.y, rec.r1.z),
                    r2 = f3(rec.r2.x, rec.r2.y, rec.r2.z);
             float gcol = r.g.x * col4.x + r.g.y * col4.y + r.g.z * col4.z;
             float gc = 0.f, dd = 0.f;
-            float3 dsc = f3(0.f, 0.f, 0.f), dp = f3(0.f, 0.f, 0.f);
-            float3 d1 = f3(0.f, 0.f, 0.f), d2 = f3(0.f, 0.f, 0.f), d3 = f3(0.f, 0.f, 0.f);
-            // Moment form: with sample positions v_i = v0 + x_i vb and m_i = m0 + x_i mb, every
-            // gradient is linear in U_k = sum_i u_i x_i^k (k = 0, 1, 2), u_i = dens * h_i * w_i.
-            // Fast arithmetic: x_i = i, vb = dt * dir.  Parity: x_i = t_i - tb, vb = dir (random
-            // sample offsets included); its weights and threshold decisions are the reference's.
+            // Moment form.  With the sample offsets from the Gaussian v_i = v0 + x_i vb, every
+            // geometric gradient of this (ray, Gaussian, slab) is linear in the ray-independent
+            // moments S1 = sum_i u_i v_i and M2 = sum_i u_i v_i v_i^T (u_i = dens * h_i * w_i), which
+            // follow from U_k = sum_i u_i x_i^k (k = 0, 1, 2).  The moments of all rays and slabs are
+            // summed per Gaussian and turned into position/scale/rotation gradients once per
+            // Gaussian afterwards (k_moment_grads).  Fast arithmetic: x_i = i, vb = dt * dir.  Parity:
+            // x_i = t_i - tb, vb = dir (random sample offsets included), the reference's weights and
+            // threshold decisions.
             const float3 v0 = (r.o + r.d * r.tb) - mu;
             const float3 vb = FAST ? r.d * kDt : r.d;
-            const float3 m0 = f3(dot3(r0, v0), dot3(r1, v0), dot3(r2, v0));
-            const float3 mb = f3(dot3(r0, vb), dot3(r1, vb), dot3(r2, vb));
             float U0 = 0.f, U1 = 0.f, U2 = 0.f;
             if (FAST) {
                 // dw_i = dens * w_i in the exponent domain (as in the forward); accumulates
                 // sum dw F, sum dw h and the moments of u = dw h, then divides by dens once
+                const float3 m0 = f3(dot3(r0, v0), dot3(r1, v0), dot3(r2, v0));
+                const float3 mb = f3(dot3(r0, vb), dot3(r1, vb), dot3(r2, vb));
                 float A = fmaf(kNegHalfLog2e, dot3(m0, m0), lg2_approx(dn));
                 float B2 = (2.f * kNegHalfLog2e) * dot3(m0, mb), Cq = kNegHalfLog2e * dot3(mb, mb);
 #pragma unroll
@@ -739,28 +739,17 @@ __device__ __forceinline__ void slab_adjoint(const WarpSmem<FAST, CAP>& sm, int 
                 gc *= dn;
                 U0 *= dn; U1 *= dn; U2 *= dn;
             }
-            {
-                float3 Sm = m0 * U0 + mb * U1;
-                float3 Smm = f3(m0.x * m0.x * U0 + 2.f * m0.x * mb.x * U1 + mb.x * mb.x * U2,
-                                m0.y * m0.y * U0 + 2.f * m0.y * mb.y * U1 + mb.y * mb.y * U2,
-                                m0.z * m0.z * U0 + 2.f * m0.z * mb.z * U1 + mb.z * mb.z * U2);
-                const float3 is = FAST ? f3(__fdividef(1.f, s4.x), __fdividef(1.f, s4.y), __fdividef(1.f, s4.z))
-                                       : f3(1.f / s4.x, 1.f / s4.y, 1.f / s4.z);
-                dsc = f3(Smm.x * is.x, Smm.y * is.y, Smm.z * is.z);
-                dp = f3(r0.x * Sm.x + r1.x * Sm.y + r2.x * Sm.z, r0.y * Sm.x + r1.y * Sm.y + r2.y * Sm.z,
-                        r0.z * Sm.x + r1.z * Sm.y + r2.z * Sm.z);
-                // P[:, j] = sum_i u_i v_i m_ij
-                float3 P0 = v0 * (m0.x * U0 + mb.x * U1) + vb * (m0.x * U1 + mb.x * U2);
-                float3 P1 = v0 * (m0.y * U0 + mb.y * U1) + vb * (m0.y * U1 + mb.y * U2);
-                float3 P2 = v0 * (m0.z * U0 + mb.z * U1) + vb * (m0.z * U1 + mb.z * U2);
-                d1 = P0 * (-is.x);
-                d2 = P1 * (-is.y);
-                d3 = P2 * (-is.z);
-            }
-            float4 dq = quat_grad(q4, d1, d2, d3);
-            v[0] = dd; v[1] = dp.x; v[2] = dp.y; v[3] = dp.z;
-            v[4] = dsc.x; v[5] = dsc.y; v[6] = dsc.z;
-            v[7] = dq.x; v[8] = dq.y; v[9] = dq.z; v[10] = dq.w;
+            // S1 = v0 U0 + vb U1; M2 = v0 v0^T U0 + (v0 vb^T + vb v0^T) U1 + vb vb^T U2
+            const float3 p = v0 * U0 + vb * U1;     // sum u v
+            const float3 q = v0 * U1 + vb * U2;     // sum u x v
+            v[0] = dd;
+            v[1] = p.x; v[2] = p.y; v[3] = p.z;
+            v[4] = v0.x * p.x + vb.x * q.x;         // xx
+            v[5] = v0.y * p.y + vb.y * q.y;         // yy
+            v[6] = v0.z * p.z + vb.z * q.z;         // zz
+            v[7] = v0.x * p.y + vb.x * q.y;         // xy
+            v[8] = v0.x * p.z + vb.x * q.z;         // xz
+            v[9] = v0.y * p.z + vb.y * q.z;         // yz
             v[11] = r.g.x * gc; v[12] = r.g.y * gc; v[13] = r.g.z * gc;
         }
         float* gg = reinterpret_cast<float*>(a.gacc_geo + 3 * (long long)leaf);
@@ -1138,6 +1127,42 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, min_blocks<BWD, FAST>()) 
         atomicAdd(&a.st->hit_pairs, sm.cnt[7]);
         atomicAdd(&a.st->slabs, sm.cnt[8]);
     }
+}
+
+// Per-leaf conversion of the summed adjoint moments into gradients (one thread per leaf):
+//   in  [dens grad, S1.xyz, M2 xx yy zz xy xz yz, 0, 0]
+//   out [dens grad, dpos.xyz, dscale.xyz, dquat.xyzw, 0]
+// with m = M v (rows of M = R^T / s): dpos = M^T M S1, dscale_j = r_j^T M2 r_j / s_j and, for the
+// rotation, P_j = M2 r_j enters the quaternion derivative as -P_j / s_j.
+__global__ void k_moment_grads(int n, const LeafRec* __restrict__ rec, const float4* __restrict__ ext,
+                               float4* __restrict__ acc) {
+    int l = blockIdx.x * blockDim.x + threadIdx.x;
+    if (l >= n) return;
+    const float4 a0 = acc[3 * (long long)l], a1 = acc[3 * (long long)l + 1], a2 = acc[3 * (long long)l + 2];
+    const LeafRec rr = rec[l];
+    const float4 s4 = ext[2 * (long long)l], q4 = ext[2 * (long long)l + 1];
+    const float3 r0 = f3(rr.r0.x, rr.r0.y, rr.r0.z), r1 = f3(rr.r1.x, rr.r1.y, rr.r1.z),
+                 r2 = f3(rr.r2.x, rr.r2.y, rr.r2.z);
+    const float3 S1 = f3(a0.y, a0.z, a0.w);
+    const float xx = a1.x, yy = a1.y, zz = a1.z, xy = a1.w, xz = a2.x, yz = a2.y;
+    auto m2 = [&](float3 w) {
+        return f3(xx * w.x + xy * w.y + xz * w.z, xy * w.x + yy * w.y + yz * w.z, xz * w.x + yz * w.y + zz * w.z);
+    };
+    const float3 Sm = f3(dot3(r0, S1), dot3(r1, S1), dot3(r2, S1));
+    const float3 dp = r0 * Sm.x + r1 * Sm.y + r2 * Sm.z;
+    const float3 P0 = m2(r0), P1 = m2(r1), P2 = m2(r2);
+    const float3 is = f3(1.f / s4.x, 1.f / s4.y, 1.f / s4.z);
+    const float3 dsc = f3(dot3(r0, P0) * is.x, dot3(r1, P1) * is.y, dot3(r2, P2) * is.z);
+    const float4 dq = quat_grad(q4, P0 * (-is.x), P1 * (-is.y), P2 * (-is.z));
+    acc[3 * (long long)l] = make_float4(a0.x, dp.x, dp.y, dp.z);
+    acc[3 * (long long)l + 1] = make_float4(dsc.x, dsc.y, dsc.z, dq.x);
+    acc[3 * (long long)l + 2] = make_float4(dq.y, dq.z, dq.w, 0.f);
+}
+
+cudaError_t launch_moment_grads(int n, const LeafRec* rec, const float4* ext, float4* acc, cudaStream_t s) {
+    if (n <= 0) return cudaSuccess;
+    k_moment_grads<<<(n + 255) / 256, 256, 0, s>>>(n, rec, ext, acc);
+    return cudaGetLastError();
 }
 
 int render_block_threads() { return kWarpsPerBlock * 32; }
