@@ -5,6 +5,8 @@
 // render_optix.py:105-106; the BVH replaces the OptiX GAS built by optix_utils.py:68-75.
 #include <cub/device/device_radix_sort.cuh>
 
+#include <climits>
+
 #include "rg_common.cuh"
 #include "rg_kernels.h"
 
@@ -257,6 +259,41 @@ __global__ void k_refit(int n, const float4* __restrict__ leaf_lo, const float4*
     }
 }
 
+// 4-wide traversal nodes.  Every internal node i at even depth gets the four grandchildren under
+// its two children as two halves in the binary node format (half 0 under the left child, half 1
+// under the right one): an internal child contributes its own node (both child boxes, ids and
+// leaf ranges), a leaf child contributes itself in slot 0 of its half and an empty slot 1 whose
+// range end (INT_MIN) never passes the traversal's cursor test.  Children stay in leaf order.
+// Internal grandchildren are at even depth again, so the 4-wide tree is indexed by binary index.
+__global__ void k_collapse(int n, const Node* __restrict__ nodes, const int* __restrict__ node_parent,
+                           Node* __restrict__ nodes4) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n - 1) return;
+    int odd = 0;
+    int p = i;
+    for (int k = 0; k < 4096; ++k) {
+        p = node_parent[p];
+        if (p < 0) break;
+        odd ^= 1;
+    }
+    if (odd) return;
+    const Node nd = nodes[i];
+    const float* f = reinterpret_cast<const float*>(&nd);
+    for (int h = 0; h < 2; ++h) {
+        const int c = h == 0 ? nd.n3.x : nd.n3.y;
+        Node half;
+        if (c >= 0) {
+            half = nodes[c];
+        } else {
+            float* hf = reinterpret_cast<float*>(&half);
+            for (int k = 0; k < 6; ++k) hf[k] = f[6 * h + k];
+            for (int k = 6; k < 12; ++k) hf[k] = 0.f;
+            half.n3 = make_int4(c, c, h == 0 ? nd.n3.z : nd.n3.w, INT_MIN);
+        }
+        nodes4[2 * (long long)i + h] = half;
+    }
+}
+
 // ---- host launchers --------------------------------------------------------------------------
 
 cudaError_t launch_prepass(const rg_gaussians* g, GaussRec* rec, float* aabb, int* scene_ord, DevStatus* st,
@@ -307,6 +344,10 @@ cudaError_t launch_refit_only(long long n, BvhBuffers& b, cudaStream_t s) {
     int blocks = (int)((n + 255) / 256);
     k_refit<<<blocks, 256, 0, s>>>((int)n, b.leaf_lo, b.leaf_hi, b.nodes, b.leaf_parent, b.node_parent, b.refit_cnt,
                                    b.root_box);
+    if (n > 1) {
+        int ib = (int)((n - 1 + 255) / 256);
+        k_collapse<<<ib, 256, 0, s>>>((int)n, b.nodes, b.node_parent, b.nodes4);
+    }
     return cudaGetLastError();
 }
 

@@ -84,6 +84,7 @@ int ensure_n(rg_engine* e, long long n) {
     if ((rc = grow(e, e->bvh.leaf_lo, N))) return rc;
     if ((rc = grow(e, e->bvh.leaf_hi, N))) return rc;
     if ((rc = grow(e, e->bvh.nodes, N > 1 ? N - 1 : 1))) return rc;
+    if ((rc = grow(e, e->bvh.nodes4, N > 1 ? 2 * (N - 1) : 2))) return rc;
     if ((rc = grow(e, e->bvh.leaf_parent, N))) return rc;
     if ((rc = grow(e, e->bvh.node_parent, N > 1 ? N - 1 : 1))) return rc;
     if ((rc = grow(e, e->bvh.refit_cnt, N > 1 ? N - 1 : 1))) return rc;
@@ -184,7 +185,7 @@ int fill_args(rg_engine* e, const rg_camera* cams, const rg_settings* s, rg::Ren
     a.is_rec = e->bvh.leaf_is;
     a.ext = e->bvh.leaf_ext;
     a.rgb = e->rgb_leaf;
-    a.nodes = e->bvh.nodes;
+    a.nodes4 = e->bvh.nodes4;
     a.n_leaves = (int)e->n_built;
     a.scene_ord = e->scene_ord;
     a.white_bg = s->white_background;
@@ -245,6 +246,7 @@ int rg_destroy(rg_engine* e) {
     set_device(e);
     void* ptrs[] = {e->rec, e->aabb, e->scene_ord, e->bvh.keys_in, e->bvh.keys_out, e->bvh.vals_in, e->bvh.leaf_gid,
                     e->bvh.rank, e->bvh.leaf_rec, e->bvh.leaf_is, e->bvh.leaf_ext, e->bvh.leaf_lo, e->bvh.leaf_hi, e->bvh.nodes,
+                    e->bvh.nodes4,
                     e->bvh.leaf_parent, e->bvh.node_parent, e->bvh.refit_cnt, e->bvh.root_box, e->bvh.sort_temp,
                     e->rgb_leaf, e->gacc_geo, e->gacc_rgb, e->vt, e->work_counter, e->st, e->rec_arena,
                     e->rec_top, e->rec_tile};

@@ -17,6 +17,7 @@ struct BvhBuffers {
     float4* leaf_lo = nullptr;
     float4* leaf_hi = nullptr;
     Node* nodes = nullptr;
+    Node* nodes4 = nullptr;       // 4-wide traversal nodes: two binary-format halves per binary node
     int* leaf_parent = nullptr;
     int* node_parent = nullptr;
     unsigned* refit_cnt = nullptr;
@@ -32,7 +33,7 @@ struct RenderArgs {
     const LeafIS* is_rec;
     const float4* ext;
     const float4* rgb;            // (n_views, n_leaves) leaf order
-    const Node* nodes;
+    const Node* nodes4;           // 4-wide traversal nodes (halves 2i, 2i+1 of internal node i)
     int n_leaves;
     const int* scene_ord;
     int white_bg, jitter, rnd_sample, max_prim_slice;

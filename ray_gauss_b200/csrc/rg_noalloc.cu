@@ -5,7 +5,7 @@
 // or plugins loaded into a process whose allocator must not be touched.  This entry point runs
 // the same pre-pass, LBVH build, colour pass and forward launch as rg_render_forward without an
 // engine and without allocating: all of its scratch lives in one file-scope device array of
-// kNoAllocScratchBytes (about 9 MB), which every GPU that loads this library holds until the
+// kNoAllocScratchBytes (about 11 MB), which every GPU that loads this library holds until the
 // process exits.  The caller still passes the Gaussians, cameras and output buffers.
 //
 // Limits: at most kNoAllocMaxGaussians (16384) Gaussians and kNoAllocMaxViews (4) views per call;
@@ -32,7 +32,7 @@ constexpr size_t align256(size_t x) { return (x + 255) & ~size_t(255); }
 // Byte offsets of every scratch buffer inside the array.
 struct NoAllocLayout {
     size_t rec, aabb, scene, keys_in, keys_out, vals_in, leaf_gid, rank, leaf_rec, leaf_is, leaf_ext, leaf_lo,
-        leaf_hi, nodes, leaf_parent, node_parent, refit_cnt, root_box, rgb_leaf, vt, work, status, sort, total;
+        leaf_hi, nodes, nodes4, leaf_parent, node_parent, refit_cnt, root_box, rgb_leaf, vt, work, status, sort, total;
 };
 
 constexpr NoAllocLayout make_layout() {
@@ -58,6 +58,7 @@ constexpr NoAllocLayout make_layout() {
     L.leaf_lo = take(sizeof(float4) * N);
     L.leaf_hi = take(sizeof(float4) * N);
     L.nodes = take(sizeof(rg::Node) * N);
+    L.nodes4 = take(sizeof(rg::Node) * 2 * N);
     L.leaf_parent = take(sizeof(int) * N);
     L.node_parent = take(sizeof(int) * N);
     L.refit_cnt = take(sizeof(unsigned) * N);
@@ -156,6 +157,7 @@ extern "C" RG_API int rg_render_forward_noalloc(const rg_gaussians* g, const rg_
     bvh.leaf_lo = at<float4>(b, kLayout.leaf_lo);
     bvh.leaf_hi = at<float4>(b, kLayout.leaf_hi);
     bvh.nodes = at<rg::Node>(b, kLayout.nodes);
+    bvh.nodes4 = at<rg::Node>(b, kLayout.nodes4);
     bvh.leaf_parent = at<int>(b, kLayout.leaf_parent);
     bvh.node_parent = at<int>(b, kLayout.node_parent);
     bvh.refit_cnt = at<unsigned>(b, kLayout.refit_cnt);
@@ -181,7 +183,7 @@ extern "C" RG_API int rg_render_forward_noalloc(const rg_gaussians* g, const rg_
     a.is_rec = bvh.leaf_is;
     a.ext = bvh.leaf_ext;
     a.rgb = rgb_leaf;
-    a.nodes = bvh.nodes;
+    a.nodes4 = bvh.nodes4;
     a.n_leaves = (int)n;
     a.scene_ord = scene_ord;
     a.white_bg = s->white_background;

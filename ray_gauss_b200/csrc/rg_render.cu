@@ -385,29 +385,35 @@ __device__ int traverse(WarpSmem<FAST, CAP>& sm, const RenderArgs& a, const RayS
             break;
         }
         if (cur >= 0) {
+            // 4-wide node: two halves in the binary node format, children in leaf order
             ++visits;
-            float lb[6], rb[6];
-            int4 n3;
-            load_node(a.nodes + cur, lb, rb, n3);
-            // non-short-circuit predicates: no branches before the ballots
-            const bool hl = box_hit<FAST>(lb, r, r.tb, seg_hi) & on & (n3.z > cursor);
-            const bool hr = box_hit<FAST>(rb, r, r.tb, seg_hi) & on & (n3.w > cursor);
-            const unsigned bl = __ballot_sync(kFull, hl), br = __ballot_sync(kFull, hr);
-            if (bl) {
-                if (br) {
-                    // every lane stores the same value and reads back only its own stores: the
-                    // stack needs neither a single writer nor a warp barrier
-                    if (sp < kStack) {
-                        sm.stack[sp] = n3.y;
-                        ++sp;
-                    } else if (lane == 0) {
-                        atomicAdd(&a.st->stack_overflows, 1ull);
-                    }
+            const Node* np = a.nodes4 + 2 * (long long)cur;
+            float ab0[6], ab1[6], bb0[6], bb1[6];
+            int4 na, nb;
+            load_node(np, ab0, ab1, na);
+            load_node(np + 1, bb0, bb1, nb);
+            // non-short-circuit predicates: no branches before the vote
+            const unsigned bits = (unsigned)(box_hit<FAST>(ab0, r, r.tb, seg_hi) & (na.z > cursor)) |
+                                  ((unsigned)(box_hit<FAST>(ab1, r, r.tb, seg_hi) & (na.w > cursor)) << 1) |
+                                  ((unsigned)(box_hit<FAST>(bb0, r, r.tb, seg_hi) & (nb.z > cursor)) << 2) |
+                                  ((unsigned)(box_hit<FAST>(bb1, r, r.tb, seg_hi) & (nb.w > cursor)) << 3);
+            const unsigned hm = __reduce_or_sync(kFull, on ? bits : 0u);
+            if (hm) {
+                // continue with the first hit child; the later ones wait on the stack, last on
+                // the bottom.  Every lane stores the same value and reads back only its own
+                // stores: the stack needs neither a single writer nor a warp barrier.
+                const int f = __ffs(hm) - 1;
+                const int more = __popc(hm) - 1;
+                if (sp + more <= kStack) {
+                    if ((hm & 8u) && f < 3) sm.stack[sp++] = nb.y;
+                    if ((hm & 4u) && f < 2) sm.stack[sp++] = nb.x;
+                    if ((hm & 2u) && f < 1) sm.stack[sp++] = na.y;
+                } else if (lane == 0) {
+                    atomicAdd(&a.st->stack_overflows, 1ull);
                 }
-                cur = n3.x;
+                cur = f == 0 ? na.x : f == 1 ? na.y : f == 2 ? nb.x : nb.y;
                 continue;
             }
-            if (br) { cur = n3.y; continue; }
         } else {
             int leaf = ~cur;
             if (leaf > cursor && !leaf_entry<FAST, CAP>(sm, a, r, on, seg_hi, K, nv, leaf, count, lane, ws)) {
