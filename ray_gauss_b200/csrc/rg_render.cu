@@ -45,7 +45,10 @@ constexpr float kNegHalfLog2e = -0.72134752044448170f;
 constexpr float kLog2SigThr = -3.3219280948873623f;   // log2(0.1): per-sample density threshold
 constexpr float kInvSlab = 50.0f;          // 1 / 0.02
 constexpr int kExactChunk = 8;             // chunks up to this length use exact slab ranges
-constexpr int kCounters = 9;               // per-warp counters: the WarpStats fields, hit pairs, slabs
+constexpr int kCounters = 9;
+#ifndef RG_DIRECT_ATOMIC_LANES
+#define RG_DIRECT_ATOMIC_LANES 16  // up to this many contributing lanes add with float4 atomics directly
+#endif               // per-warp counters: the WarpStats fields, hit pairs, slabs
 constexpr unsigned kNoRecord = 0xffffffffu;     // hit-list record: no (next) chunk record
 constexpr unsigned kRecordMulti = 0x80000000u;  // chunk consumed in several traversal passes
 constexpr unsigned kRecordFailed = 0xfffffffeu; // the tile's record did not fit the arena
@@ -760,8 +763,13 @@ __device__ __forceinline__ void slab_adjoint(const WarpSmem<FAST, CAP>& sm, int 
         }
         float* gg = reinterpret_cast<float*>(a.gacc_geo + 3 * (long long)leaf);
         float* gr = reinterpret_cast<float*>(a.gacc_rgb + rgb_base + leaf);
-        if (__popc(am) == 1) {
-            if (act) {
+        // lanes whose samples all fell under the threshold contribute nothing
+        const bool nz = act && (v[0] != 0.f || v[1] != 0.f || v[2] != 0.f || v[3] != 0.f || v[11] != 0.f ||
+                                v[12] != 0.f || v[13] != 0.f);
+        const unsigned zm = __ballot_sync(kFull, nz);
+        if (zm == 0u) continue;
+        if (__popc(zm) <= RG_DIRECT_ATOMIC_LANES) {
+            if (nz) {
                 float4* g4 = reinterpret_cast<float4*>(gg);
                 atomicAdd(g4, make_float4(v[0], v[1], v[2], v[3]));
                 atomicAdd(g4 + 1, make_float4(v[4], v[5], v[6], v[7]));
