@@ -216,6 +216,13 @@ __device__ __forceinline__ bool slab_hit_exact(const RenderArgs& a, int leaf, fl
 }
 
 // Slab range [lo, hi] of the chunk (K slabs from r.tb) hit by the interval [root1, root2].
+// Longer chunks map the interval arithmetically.  Slab k starts at tb_k, tb plus k slabs by repeated
+// FP32 addition, and is hit iff root1 <= tb_k + 0.02 and tb_k <= root2.  The parity arithmetic keeps
+// one slab of margin on each side (its end slabs are re-decided by the exact test); the fast
+// arithmetic keeps only a margin that covers the drift of the repeated addition (K additions of at
+// most one ulp each), since samples of a slab the interval misses fall outside the threshold
+// ellipsoid anyway.
+template <bool FAST>
 __device__ __forceinline__ void slab_range(const RayState& r, int K, int nv, float seg_hi, float root1, float root2,
                                            int& lo, int& hi) {
     lo = 255;
@@ -238,8 +245,15 @@ __device__ __forceinline__ void slab_range(const RayState& r, int K, int nv, flo
     } else if (fmaxf(r.tb, root1) <= fminf(seg_hi, root2)) {
         float a = fmaxf((root1 - r.tb) * kInvSlab, -1.f);
         float b = fminf((root2 - r.tb) * kInvSlab, 4096.f);
-        lo = max(0, (int)floorf(a) - 1);
-        hi = min(K - 1, (int)floorf(b) + 1);
+        if (FAST) {
+            // drift of tb_k in slab units: (K + 1) ulps of |tb| + K slabs, 2^-23 relative each
+            const float m = (float)(K + 1) * (fabsf(r.tb) + (float)K * kSlab) * (kInvSlab * 2.4e-7f) + 1e-4f;
+            lo = max(0, (int)ceilf(a - 1.f - m));
+            hi = min(K - 1, (int)floorf(b + m));
+        } else {
+            lo = max(0, (int)floorf(a) - 1);
+            hi = min(K - 1, (int)floorf(b) + 1);
+        }
         if (lo > hi) { lo = 255; hi = -1; }
     }
 }
@@ -321,7 +335,7 @@ __device__ __forceinline__ bool leaf_entry(WarpSmem<FAST, CAP>& sm, const Render
             float4 m4 = __ldg(reinterpret_cast<const float4*>(a.rec + leaf));
             ok = roots_exact(load_is(a.is_rec, leaf), f3(m4.x, m4.y, m4.z), r, root1, root2);
         }
-        if (ok) slab_range(r, K, nv, seg_hi, root1, root2, lo, hi);
+        if (ok) slab_range<FAST>(r, K, nv, seg_hi, root1, root2, lo, hi);
     }
     unsigned any = __ballot_sync(kFull, lo <= hi);
     if (!any) return true;
