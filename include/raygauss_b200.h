@@ -146,7 +146,8 @@ typedef struct rg_status {
 typedef struct rg_tuning {
     int32_t chunk_slabs;               /* longest traversal chunk in slabs, 1..255 */
     int32_t blocks_per_sm;             /* resident render CTAs per SM */
-    int32_t list_capacity;             /* warp hit-list capacity: 64 or 128 */
+    int32_t list_capacity;             /* 64 or 128: fast-arithmetic warp hit lists hold 4x this
+                                          many entries; parity lists always hold 128 */
     int32_t record_hits;               /* 1: the forward records its hit lists and the backward
                                           replays them (default); -1: the backward traverses */
 } rg_tuning;

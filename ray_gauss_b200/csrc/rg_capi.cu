@@ -170,6 +170,11 @@ int set_device(rg_engine* e) {
     return RG_OK;
 }
 
+// The fast kernels run only without random sample offsets (launch_render picks the same way).
+int kernel_mode(const rg_settings* s) {
+    return (s->mode == RG_MODE_FAST && s->rnd_sample == 0) ? RG_MODE_FAST : RG_MODE_PARITY;
+}
+
 int render_grid(rg_engine* e, bool bwd, int mode) {
     int per_sm = e->tuning.blocks_per_sm;
     int occ = rg::render_occupancy(bwd, mode, e->tuning.list_capacity);
@@ -377,7 +382,7 @@ int rg_launch_forward(rg_engine* e, const rg_camera* cams, int32_t n_cams, const
         a.rec_tile = e->rec_tile;
         a.rec_tiles = e->rec_tiles;
     }
-    int grid = render_grid(e, false, s->mode);
+    int grid = render_grid(e, false, kernel_mode(s));
     RG_CUDA(rg::launch_render(false, s->mode, e->tuning.list_capacity, grid, a, S(stream)), "render forward");
     e->launches += 2;
     if (record) {
@@ -417,7 +422,7 @@ int rg_launch_backward(rg_engine* e, const rg_camera* cams, int32_t n_cams, cons
         a.rec_tiles = e->rec_tiles;
         a.replay = 1;
     }
-    int grid = render_grid(e, true, s->mode);
+    int grid = render_grid(e, true, kernel_mode(s));
     RG_CUDA(rg::launch_render(true, s->mode, e->tuning.list_capacity, grid, a, S(stream)), "render backward");
     RG_CUDA(rg::launch_moment_grads((int)N, e->bvh.leaf_rec, e->bvh.leaf_ext, e->gacc_geo, S(stream)), "moments");
     e->launches += 3;

@@ -217,11 +217,10 @@ __device__ __forceinline__ bool slab_hit_exact(const RenderArgs& a, int leaf, fl
 
 // Slab range [lo, hi] of the chunk (K slabs from r.tb) hit by the interval [root1, root2].
 // Longer chunks map the interval arithmetically.  Slab k starts at tb_k, tb plus k slabs by repeated
-// FP32 addition, and is hit iff root1 <= tb_k + 0.02 and tb_k <= root2.  The parity arithmetic keeps
-// one slab of margin on each side (its end slabs are re-decided by the exact test); the fast
-// arithmetic keeps only a margin that covers the drift of the repeated addition (K additions of at
-// most one ulp each), since samples of a slab the interval misses fall outside the threshold
-// ellipsoid anyway.
+// FP32 addition, and is hit iff root1 <= tb_k + 0.02 and tb_k <= root2.  The range keeps a margin
+// that covers the drift of the repeated addition, so it holds every hit slab and at most one extra
+// slab at each end: the parity arithmetic re-decides the two end slabs with the exact test, the fast
+// arithmetic evaluates them (their samples fall outside the threshold ellipsoid).
 template <bool FAST>
 __device__ __forceinline__ void slab_range(const RayState& r, int K, int nv, float seg_hi, float root1, float root2,
                                            int& lo, int& hi) {
@@ -245,15 +244,11 @@ __device__ __forceinline__ void slab_range(const RayState& r, int K, int nv, flo
     } else if (fmaxf(r.tb, root1) <= fminf(seg_hi, root2)) {
         float a = fmaxf((root1 - r.tb) * kInvSlab, -1.f);
         float b = fminf((root2 - r.tb) * kInvSlab, 4096.f);
-        if (FAST) {
-            // drift of tb_k in slab units: (K + 1) ulps of |tb| + K slabs, 2^-23 relative each
-            const float m = (float)(K + 1) * (fabsf(r.tb) + (float)K * kSlab) * (kInvSlab * 2.4e-7f) + 1e-4f;
-            lo = max(0, (int)ceilf(a - 1.f - m));
-            hi = min(K - 1, (int)floorf(b + m));
-        } else {
-            lo = max(0, (int)floorf(a) - 1);
-            hi = min(K - 1, (int)floorf(b) + 1);
-        }
+        // drift of tb_k in slab units: (K + 1) ulps of |tb| + K slabs, 2^-23 relative each (four
+        // times the bound of round-to-nearest additions)
+        const float m = (float)(K + 1) * (fabsf(r.tb) + (float)K * kSlab) * (kInvSlab * 2.4e-7f) + 1e-4f;
+        lo = max(0, (int)ceilf(a - 1.f - m));
+        hi = min(K - 1, (int)floorf(b + m));
         if (lo > hi) { lo = 255; hi = -1; }
     }
 }
@@ -514,9 +509,9 @@ __device__ __forceinline__ bool in_urange(unsigned u, int k) {
 }
 
 // Whether lane-entry range rg holds slab k.  Chunks longer than kExactChunk carry conservative
-// ranges; in the parity arithmetic the two slabs at each end are decided by the reference's exact
-// per-slab test (the extra slabs' samples lie outside the threshold ellipsoid, but only up to the
-// rounding of the intersection arithmetic).
+// ranges (every hit slab, at most one extra slab at each end); in the parity arithmetic the end
+// slabs are decided by the reference's exact per-slab test (an extra slab's samples lie outside
+// the threshold ellipsoid, but only up to the rounding of the intersection arithmetic).
 template <bool FAST, int CAP>
 __device__ __forceinline__ bool lane_has_entry(const WarpSmem<FAST, CAP>& sm, const RenderArgs& a, int e, int k, int K,
                                                int leaf, const RayState& r, int lane) {
@@ -524,7 +519,7 @@ __device__ __forceinline__ bool lane_has_entry(const WarpSmem<FAST, CAP>& sm, co
     unsigned short rg = sm.lrng[e][lane];
     int lo = rg & 0xff, hi = rg >> 8;
     if (k < lo || k > hi) return false;
-    if (K <= kExactChunk || (k > lo + 1 && k < hi - 1)) return true;
+    if (K <= kExactChunk || (k > lo && k < hi)) return true;
     float4 m4 = __ldg(reinterpret_cast<const float4*>(a.rec + leaf));
     return slab_hit_exact(a, leaf, f3(m4.x, m4.y, m4.z), r);
 }
@@ -1195,9 +1190,10 @@ cudaError_t launch_moment_grads(int n, const LeafRec* rec, const float4* ext, fl
 
 int render_block_threads() { return kWarpsPerBlock * 32; }
 
-// List capacity per arithmetic: the tuning value (64 or 128) for parity, 4x for fast.
+// List capacity per arithmetic: 4x the tuning value (64 or 128) for the fast lists; 128 for the
+// parity lists at either value (their per-lane slab ranges make an entry 64 B; shorter lists turn
+// dense slabs into multi-pass traversals, which the backward cannot replay).
 size_t render_smem_bytes(bool, int cap) {
-    if (cap <= 64) return sizeof(WarpSmem<false, 64>) * kWarpsPerBlock;
     return sizeof(WarpSmem<false, 128>) * kWarpsPerBlock;
 }
 static_assert(sizeof(WarpSmem<false, 128>) * kWarpsPerBlock <= 48 * 1024, "static shared memory limit");
@@ -1210,8 +1206,7 @@ static cudaError_t launch_cap(int cap, int grid, const RenderArgs& a, cudaStream
         if (cap <= 64) k_render<BWD, FAST, 256><<<grid, threads, 0, s>>>(a);
         else k_render<BWD, FAST, 512><<<grid, threads, 0, s>>>(a);
     } else {
-        if (cap <= 64) k_render<BWD, FAST, 64><<<grid, threads, 0, s>>>(a);
-        else k_render<BWD, FAST, 128><<<grid, threads, 0, s>>>(a);
+        k_render<BWD, FAST, 128><<<grid, threads, 0, s>>>(a);
     }
     return cudaGetLastError();
 }
@@ -1224,8 +1219,7 @@ static int occ_cap(int cap) {
         if (cap <= 64) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_render<BWD, FAST, 256>, threads, 0);
         else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_render<BWD, FAST, 512>, threads, 0);
     } else {
-        if (cap <= 64) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_render<BWD, FAST, 64>, threads, 0);
-        else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_render<BWD, FAST, 128>, threads, 0);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_render<BWD, FAST, 128>, threads, 0);
     }
     return nb;
 }
