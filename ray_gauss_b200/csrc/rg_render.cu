@@ -90,8 +90,9 @@ struct RayState {
     float tenter, texit;
     float tb;
     float T;
-    float3 C;     // forward: accumulated colour; backward: remaining colour R
+    float3 C;     // forward: accumulated colour
     float3 g;     // backward: dL/dcolour of the ray
+    float gR;     // backward: g . R, R the colour still to come (the adjoint needs only this product)
     unsigned seed;
     bool alive;
 };
@@ -524,11 +525,12 @@ __device__ __forceinline__ bool lane_has_entry(const WarpSmem<FAST, CAP>& sm, co
     return slab_hit_exact(a, leaf, f3(m4.x, m4.y, m4.z), r);
 }
 
-// Sample buffers of slab k: sum of density and density-weighted colour of the lane's hits.
-template <bool FAST, int CAP>
+// Sample buffers of slab k: sum of density and density-weighted colour of the lane's hits.  The
+// backward (GDOT) needs the colour only through g . C, so it accumulates that scalar in gC instead.
+template <bool FAST, int CAP, bool GDOT>
 __device__ __forceinline__ int slab_buffers(const WarpSmem<FAST, CAP>& sm, int k, int K, bool has, const RayState& r,
                                             const RenderArgs& a, int rgb_base, const float* roff,
-                                            float* sig, float3* C, int nw, int lane, WarpStats& ws) {
+                                            float* sig, float3* C, float* gC, int nw, int lane, WarpStats& ws) {
     int nh = 0;
 #pragma unroll 1
     for (int w = 0; w < nw; ++w) {
@@ -557,6 +559,7 @@ __device__ __forceinline__ int slab_buffers(const WarpSmem<FAST, CAP>& sm, int k
                 float A = fmaf(kNegHalfLog2e, dot3(m0, m0), lg2_approx(dn));
                 float B2 = (2.f * kNegHalfLog2e) * dot3(m0, mb), Cq = kNegHalfLog2e * dot3(mb, mb);
                 float3 col = f3(col4.x, col4.y, col4.z);
+                const float gcol = GDOT ? dot3(r.g, col) : 0.f;
 #pragma unroll
                 for (int i = 0; i < kBuf; ++i) {
                     float fi = (float)i;
@@ -564,7 +567,8 @@ __device__ __forceinline__ int slab_buffers(const WarpSmem<FAST, CAP>& sm, int k
                     if (e > kLog2SigThr) {
                         float dw = ex2_approx(e);
                         sig[i] += dw;
-                        C[i] = C[i] + col * dw;
+                        if (GDOT) gC[i] = fmaf(gcol, dw, gC[i]);
+                        else C[i] = C[i] + col * dw;
                     }
                 }
             } else {
@@ -576,9 +580,13 @@ __device__ __forceinline__ int slab_buffers(const WarpSmem<FAST, CAP>& sm, int k
                     float w = parity_weight(r.o, r.d, t, mu, r0, r1, r2, dn, v, m, in);
                     if (in) {
                         sig[i] = __fadd_rn(sig[i], __fmul_rn(dn, w));
-                        C[i] = f3(__fadd_rn(C[i].x, __fmul_rn(__fmul_rn(col4.x, w), dn)),
-                                  __fadd_rn(C[i].y, __fmul_rn(__fmul_rn(col4.y, w), dn)),
-                                  __fadd_rn(C[i].z, __fmul_rn(__fmul_rn(col4.z, w), dn)));
+                        if (GDOT) {
+                            gC[i] += (r.g.x * col4.x + r.g.y * col4.y + r.g.z * col4.z) * (w * dn);
+                        } else {
+                            C[i] = f3(__fadd_rn(C[i].x, __fmul_rn(__fmul_rn(col4.x, w), dn)),
+                                      __fadd_rn(C[i].y, __fmul_rn(__fmul_rn(col4.y, w), dn)),
+                                      __fadd_rn(C[i].z, __fmul_rn(__fmul_rn(col4.z, w), dn)));
+                        }
                     }
                 }
             }
@@ -798,28 +806,26 @@ __device__ __forceinline__ void slab_adjoint(const WarpSmem<FAST, CAP>& sm, int 
 
 // Per-sample compositing adjoint scalars of one slab (reference backward :675-730): with
 // E = g.((T c - R) dt), F = T alpha / sigma and G = g.c, a Gaussian of colour col and weight w
-// at the sample has dL/d(sigma-share) h = E + F (g.col - G) = F g.col + H, H = E - F G.
-// Returns H and F; advances T and R over the slab.
+// at the sample has dL/d(sigma-share) h = E + F (g.col - G) = F g.col + H, H = E - F G.  Only
+// g.C (gC, C the colour sum of the sample) and g.R (r.gR) enter: with gc = g.C / sigma,
+// E = dt (T gc - g.R), H = E - F gc, and g.R drops by gc T alpha per sample.
+// Returns H and F; advances T and g.R over the slab.
 template <bool FAST>
-__device__ __forceinline__ void slab_adjoint_scalars(const RayState& r, const float* sig, const float3* Cb, float* H,
-                                                     float* F, float& Ta, float3& Ra) {
+__device__ __forceinline__ void slab_adjoint_scalars(const RayState& r, const float* sig, const float* gC, float* H,
+                                                     float* F, float& Ta, float& gRa) {
     Ta = r.T;
-    Ra = r.C;
+    gRa = r.gR;
 #pragma unroll
     for (int i = 0; i < kBuf; ++i) {
-        float cd = sig[i];
-        float3 cc = Cb[i];
+        const float cd = sig[i];
         float inv = 0.f;
-        if (cd > 0.f) {
-            inv = FAST ? __fdividef(1.f, cd) : 1.f / cd;
-            cc = cc * inv;
-        }
-        float alpha = FAST ? 1.f - exp_neg<true>(cd * kDt) : __fsub_rn(1.f, exp_neg<false>(__fmul_rn(cd, kDt)));
-        float3 aux = (cc * Ta - Ra) * kDt;
-        const float Ei = dot3(r.g, aux);
-        F[i] = FAST ? Ta * alpha * inv : (cd > 0.f ? Ta * alpha / cd : 0.f);
-        H[i] = Ei - F[i] * dot3(r.g, cc);
-        Ra = Ra - cc * (Ta * alpha);
+        if (cd > 0.f) inv = FAST ? __fdividef(1.f, cd) : 1.f / cd;
+        const float gc = gC[i] * inv;
+        const float alpha = FAST ? 1.f - exp_neg<true>(cd * kDt) : __fsub_rn(1.f, exp_neg<false>(__fmul_rn(cd, kDt)));
+        const float ta = Ta * alpha;
+        F[i] = ta * inv;
+        H[i] = kDt * (Ta * gc - gRa) - F[i] * gc;
+        gRa -= gc * ta;
         Ta = FAST ? Ta * (1.f - alpha) : __fmul_rn(Ta, __fsub_rn(1.f, alpha));
     }
 }
@@ -928,10 +934,12 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, min_blocks<BWD, FAST>()) 
         r.T = 1.f;
         r.C = f3(0.f, 0.f, 0.f);
         r.g = f3(0.f, 0.f, 0.f);
+        r.gR = 0.f;
         if (BWD && valid) {
             const long long ray_g = vt->ray_prefix[view] + (long long)ray_l;
-            r.C = f3(a.ray_colors_in[3 * ray_g], a.ray_colors_in[3 * ray_g + 1], a.ray_colors_in[3 * ray_g + 2]);
             r.g = f3(a.dL[3 * ray_g], a.dL[3 * ray_g + 1], a.dL[3 * ray_g + 2]);
+            r.gR = r.g.x * a.ray_colors_in[3 * ray_g] + r.g.y * a.ray_colors_in[3 * ray_g + 1] +
+                   r.g.z * a.ray_colors_in[3 * ray_g + 2];
         }
 
         int K = min(kExactChunk, kmax);
@@ -1038,11 +1046,16 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, min_blocks<BWD, FAST>()) 
                     float roff[kBuf];
                     unsigned seed_next = slab_offsets(a.rnd_sample, r.seed, roff);
                     float sig[kBuf];
-                    float3 Cb[kBuf];
+                    float3 Cb[BWD ? 1 : kBuf];
+                    float gC[BWD ? kBuf : 1];
 #pragma unroll
-                    for (int i = 0; i < kBuf; ++i) { sig[i] = 0.f; Cb[i] = f3(0.f, 0.f, 0.f); }
-                    int nh =
-                        slab_buffers<FAST, CAP>(sm, k, K, has, r, a, rgb_base, roff, sig, Cb, nwords(count), lane, ws);
+                    for (int i = 0; i < kBuf; ++i) {
+                        sig[i] = 0.f;
+                        if (BWD) gC[i] = 0.f;
+                        else Cb[i] = f3(0.f, 0.f, 0.f);
+                    }
+                    int nh = slab_buffers<FAST, CAP, BWD>(sm, k, K, has, r, a, rgb_base, roff, sig, Cb, gC,
+                                                          nwords(count), lane, ws);
                     if (has) {
                         ++slabs_acc;
                         hits_acc += nh;
@@ -1054,14 +1067,13 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, min_blocks<BWD, FAST>()) 
                             r.seed = seed_next;
                         }
                     } else {
-                        float H[kBuf], F[kBuf], Ta;
-                        float3 Ra;
-                        slab_adjoint_scalars<FAST>(r, sig, Cb, H, F, Ta, Ra);
+                        float H[kBuf], F[kBuf], Ta, gRa;
+                        slab_adjoint_scalars<FAST>(r, sig, gC, H, F, Ta, gRa);
                         bool act = has && nh > 0 && any_density(sig);
                         slab_adjoint<FAST, CAP>(sm, k, K, act, r, a, rgb_base, roff, H, F, nwords(count), lane, ws);
                         if (has && nh > 0) {
                             r.T = Ta;
-                            r.C = Ra;
+                            r.gR = gRa;
                             r.seed = seed_next;
                         }
                     }
@@ -1078,18 +1090,24 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, min_blocks<BWD, FAST>()) 
                 float roff[kBuf];
                 unsigned seed_next = slab_offsets(a.rnd_sample, r.seed, roff);
                 float sig[kBuf];
-                float3 Cb[kBuf];
+                float3 Cb[BWD ? 1 : kBuf];
+                float gC[BWD ? kBuf : 1];
 #pragma unroll
-                for (int i = 0; i < kBuf; ++i) { sig[i] = 0.f; Cb[i] = f3(0.f, 0.f, 0.f); }
-                int nh = slab_buffers<FAST, CAP>(sm, 0, 1, has, r, a, rgb_base, roff, sig, Cb, nwords(count), lane, ws);
+                for (int i = 0; i < kBuf; ++i) {
+                    sig[i] = 0.f;
+                    if (BWD) gC[i] = 0.f;
+                    else Cb[i] = f3(0.f, 0.f, 0.f);
+                }
+                int nh = slab_buffers<FAST, CAP, BWD>(sm, 0, 1, has, r, a, rgb_base, roff, sig, Cb, gC, nwords(count),
+                                                      lane, ws);
                 bool more = ovf;
                 while (more) {
                     int cursor = sm.ids[count - 1];
                     __syncwarp();
                     if (lane == 0) atomicAdd(&a.st->list_passes, 1ull);
                     count = traverse<FAST, CAP>(sm, a, r, on, seg_hi, 1, nv, cursor, more, lane, ws);
-                    nh += slab_buffers<FAST, CAP>(sm, 0, 1, has, r, a, rgb_base, roff, sig, Cb, nwords(count), lane,
-                                                  ws);
+                    nh += slab_buffers<FAST, CAP, BWD>(sm, 0, 1, has, r, a, rgb_base, roff, sig, Cb, gC,
+                                                       nwords(count), lane, ws);
                 }
                 if (has) {
                     ++slabs_acc;
@@ -1102,9 +1120,8 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, min_blocks<BWD, FAST>()) 
                         r.seed = seed_next;
                     }
                 } else {
-                    float H[kBuf], F[kBuf], Ta;
-                    float3 Ra;
-                    slab_adjoint_scalars<FAST>(r, sig, Cb, H, F, Ta, Ra);
+                    float H[kBuf], F[kBuf], Ta, gRa;
+                    slab_adjoint_scalars<FAST>(r, sig, gC, H, F, Ta, gRa);
                     bool act = has && nh > 0 && any_density(sig);
                     int cursor = -1;
                     bool more2 = true;
@@ -1116,7 +1133,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, min_blocks<BWD, FAST>()) 
                     }
                     if (has && nh > 0) {
                         r.T = Ta;
-                        r.C = Ra;
+                        r.gR = gRa;
                         r.seed = seed_next;
                     }
                 }
