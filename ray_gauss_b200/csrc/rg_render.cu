@@ -207,21 +207,30 @@ __device__ __forceinline__ LeafIS load_is(const LeafIS* p, int i) {
     return s;
 }
 
-// The reference's per-slab test for the slab starting at r.tb (exact; used at the ends of the
-// conservative ranges of long chunks in the parity arithmetic).
-__device__ __forceinline__ bool slab_hit_exact(const RenderArgs& a, int leaf, float3 mu, const RayState& r) {
-    float root1, root2;
-    if (!roots_exact(load_is(a.is_rec, leaf), mu, r, root1, root2)) return false;
-    float th = fminf(r.texit, r.tb + kSlab);
-    return th > r.tenter && fmaxf(r.tb, root1) <= fminf(th, root2);
+// Slab range [lo, hi] of the chunk (K slabs from r.tb) hit by the interval [root1, root2].
+// Slab k of the chunk against the interval, in slab units from tb (a, b: interval ends, e: box
+// exit) with tb_k = k up to the margin m: 1 certain hit, -1 certain miss, 0 undecided.  Slab k is
+// hit iff root1 <= min(texit, tb_k + 0.02), tb_k <= root2 and root1 <= root2.
+__device__ __forceinline__ int classify_slab(int k, float a, float b, float e, float m) {
+    const float kf = (float)k;
+    if (a > b || a > kf + 1.f + m || a > e + m || kf - m > b) return -1;
+    if (a <= kf + 1.f - m && a <= e - m && kf + m <= b) return 1;
+    return 0;
 }
 
-// Slab range [lo, hi] of the chunk (K slabs from r.tb) hit by the interval [root1, root2].
+// The reference's test for slab k of the chunk, tb_k by k repeated FP32 additions from tb.
+__device__ __noinline__ bool slab_k_hit(float tb, float tenter, float texit, int k, float root1, float root2) {
+    float t = tb;
+    for (int j = 0; j < k; ++j) t = t + kSlab;
+    const float th = fminf(texit, t + kSlab);
+    return th > tenter && fmaxf(t, root1) <= fminf(th, root2);
+}
+
 // Longer chunks map the interval arithmetically.  Slab k starts at tb_k, tb plus k slabs by repeated
 // FP32 addition, and is hit iff root1 <= tb_k + 0.02 and tb_k <= root2.  The range keeps a margin
 // that covers the drift of the repeated addition, so it holds every hit slab and at most one extra
-// slab at each end: the parity arithmetic re-decides the two end slabs with the exact test, the fast
-// arithmetic evaluates them (their samples fall outside the threshold ellipsoid).
+// slab at each end: the parity arithmetic settles the ends exactly here, the fast arithmetic
+// evaluates them (their samples fall outside the threshold ellipsoid).
 template <bool FAST>
 __device__ __forceinline__ void slab_range(const RayState& r, int K, int nv, float seg_hi, float root1, float root2,
                                            int& lo, int& hi) {
@@ -250,6 +259,22 @@ __device__ __forceinline__ void slab_range(const RayState& r, int K, int nv, flo
         const float m = (float)(K + 1) * (fabsf(r.tb) + (float)K * kSlab) * (kInvSlab * 2.4e-7f) + 1e-4f;
         lo = max(0, (int)ceilf(a - 1.f - m));
         hi = min(K - 1, (int)floorf(b + m));
+        if (!FAST) {
+            // Parity: settle both ends exactly.  A slab whose hit or miss the margins cannot decide
+            // gets the reference's per-slab test (rare: its interval end lies within the margin
+            // of a slab edge or of the box exit).
+            const float e = fminf((r.texit - r.tb) * kInvSlab, 4096.f);
+            while (lo <= hi) {
+                const int c = classify_slab(lo, a, b, e, m);
+                if (c > 0 || (c == 0 && slab_k_hit(r.tb, r.tenter, r.texit, lo, root1, root2))) break;
+                ++lo;
+            }
+            while (hi >= lo) {
+                const int c = classify_slab(hi, a, b, e, m);
+                if (c > 0 || (c == 0 && slab_k_hit(r.tb, r.tenter, r.texit, hi, root1, root2))) break;
+                --hi;
+            }
+        }
         if (lo > hi) { lo = 255; hi = -1; }
     }
 }
@@ -509,20 +534,14 @@ __device__ __forceinline__ bool in_urange(unsigned u, int k) {
     return k >= (int)(u & 0xffff) && k <= (int)(u >> 16);
 }
 
-// Whether lane-entry range rg holds slab k.  Chunks longer than kExactChunk carry conservative
-// ranges (every hit slab, at most one extra slab at each end); in the parity arithmetic the end
-// slabs are decided by the reference's exact per-slab test (an extra slab's samples lie outside
-// the threshold ellipsoid, but only up to the rounding of the intersection arithmetic).
+// Whether the lane holds list entry e in slab k: the fast lists keep the lanes whose interval meets
+// the chunk, the parity lists each lane's exact slab range.
 template <bool FAST, int CAP>
 __device__ __forceinline__ bool lane_has_entry(const WarpSmem<FAST, CAP>& sm, const RenderArgs& a, int e, int k, int K,
                                                int leaf, const RayState& r, int lane) {
     if (FAST) return (sm.lmask[e] >> lane) & 1u;
-    unsigned short rg = sm.lrng[e][lane];
-    int lo = rg & 0xff, hi = rg >> 8;
-    if (k < lo || k > hi) return false;
-    if (K <= kExactChunk || (k > lo && k < hi)) return true;
-    float4 m4 = __ldg(reinterpret_cast<const float4*>(a.rec + leaf));
-    return slab_hit_exact(a, leaf, f3(m4.x, m4.y, m4.z), r);
+    const unsigned short rg = sm.lrng[e][lane];
+    return k >= (int)(rg & 0xff) && k <= (int)(rg >> 8);
 }
 
 // Sample buffers of slab k: sum of density and density-weighted colour of the lane's hits.  The
