@@ -52,7 +52,7 @@ def num_threads() -> int:
 
 
 def ref_available() -> bool:
-    return all(os.path.exists(os.path.join(_HERE, "_ref", f"libref_{s}.so")) for s in ("fwd", "bwd", "sh"))
+    return all(os.path.exists(os.path.join(_HERE, "_ref", f"libref_{s}.so")) for s in ("fwd", "bwd", "sh", "test"))
 
 
 def _ref(stage: str):
@@ -183,7 +183,50 @@ def render_backward(pos, scl, quat, dens, rgb, cam_vec, width, height, ray_color
     return g
 
 
+def render_inference(pos, scl, quat, dens, rgb, cam_vec, width, height, white_bg=True, max_prim_slice=1024,
+                     ray_ids=None, aabb=None, scene_box=None, prec="f32", order=None):
+    """Inference render (the reference's cuda_test programs): image (n_rays, 3) and Gaussians per
+    ray (n_rays,) int32."""
+    dt = _dt(prec)
+    pos, scl, quat, dens, rgb = (_c(a, dt) for a in (pos, scl, quat, dens, rgb))
+    if aabb is None or scene_box is None:
+        aabb, scene_box = bbox(pos, scl, quat, dens, prec)
+    aabb, scene_box, cam = _c(aabb, dt), _c(scene_box, dt), _c(cam_vec, dt)
+    ids = None if ray_ids is None else _c(ray_ids, np.int32)
+    order = None if order is None else _c(order, np.int32)
+    nr = width * height if ids is None else ids.shape[0]
+    out = np.zeros((nr, 3), dt)
+    counts = np.zeros(nr, np.int32)
+    stats = np.zeros(4, np.int64)
+    getattr(_lib(), "orc_render_inference_" + prec)(
+        ctypes.c_int(pos.shape[0]), _p(pos), _p(scl), _p(quat), _p(dens), _p(rgb), _p(aabb), _p(scene_box),
+        _p(cam), ctypes.c_int(width), ctypes.c_int(height), ctypes.c_int(int(bool(white_bg))),
+        ctypes.c_int(max_prim_slice), _p(ids), ctypes.c_int(nr), _p(order), _p(out), _p(counts), _p(stats))
+    return out, counts
+
+
 # ---- the reference's own device programs, compiled for the CPU (oracle/_ref) ------------------
+
+def ref_render_inference(pos, scl, quat, dens, rgb, cam_vec, width, height, white_bg=True, max_prim_slice=1024,
+                         aabb=None, scene_box=None, ray_ids=None):
+    """The reference's inference programs: image (n_rays, 3) and Gaussians per ray (n_rays,)."""
+    f = np.float32
+    pos, scl, quat, dens, rgb = (_c(a, f) for a in (pos, scl, quat, dens, rgb))
+    if aabb is None or scene_box is None:
+        aabb, scene_box = bbox(pos, scl, quat, dens, "f32")
+    aabb, scene_box, cam = _c(aabb, f), _c(scene_box, f), _c(cam_vec, f)
+    ids = None if ray_ids is None else _c(ray_ids, np.int32)
+    nr = width * height if ids is None else ids.shape[0]
+    out = np.zeros((nr, 3), f)
+    counts = np.zeros(nr, np.int32)
+    rc = _ref("test").ref_inference(
+        ctypes.c_int(pos.shape[0]), _p(pos), _p(scl), _p(quat), _p(dens), _p(rgb), _p(aabb), _p(scene_box),
+        _p(cam), ctypes.c_int(width), ctypes.c_int(height), ctypes.c_int(int(bool(white_bg))),
+        ctypes.c_int(max_prim_slice), _p(ids), ctypes.c_int(0 if ids is None else ids.shape[0]), _p(out),
+        _p(counts))
+    assert rc == 0
+    return out, counts
+
 
 def ref_render_forward(pos, scl, quat, dens, rgb, cam_vec, width, height, white_bg=True, max_prim_slice=1024,
                        jitter=0, rnd_sample=0, iteration=0, aabb=None, scene_box=None, ray_ids=None):

@@ -1,9 +1,10 @@
 /*
  * Runs the reference's own device programs on the CPU — TEST INFRASTRUCTURE ONLY.
- * oracle/Makefile compiles this file three times against sources in the reference tree
+ * oracle/Makefile compiles this file four times against sources in the reference tree
  * (REF_STAGE 1: cuda_train/forward/gaussians_aabb.cu, 2: cuda_train/backward/gaussians_aabb.cu,
- * 3: vec_math.h + utils/sh_utils.cu), with ref_shim/optix.h standing in for the OptiX device
- * API.  The outputs (oracle/_ref/*.so) pin the C restatement in rg_oracle_impl.h.
+ * 3: vec_math.h + utils/sh_utils.cu, 4: cuda_test/gaussians_aabb.cu, the inference programs),
+ * with ref_shim/optix.h standing in for the OptiX device API.  The outputs (oracle/_ref/*.so)
+ * pin the C restatement in rg_oracle_impl.h.
  */
 #include <cstring>
 #include <cstdlib>
@@ -99,6 +100,62 @@ extern "C" int ref_backward(int n, const float* pos, const float* scl, const flo
     rg_emul_scene.aabb = aabb; rg_emul_scene.n = n; rg_emul_scene.sbt_data = &g_sbt;
     run_rays(W, H, ids, n_ids);
     std::free(hit_buf);
+    return 0;
+}
+#elif REF_STAGE == 4
+#include REF_SOURCE
+thread_local RgEmulRay rg_emul;
+RgEmulScene rg_emul_scene;
+static sphere::SphereHitGroupData g_sbt;
+
+/* optix_utils.py:302-373: inference launch; colours (R,3) and Gaussians per ray (R) */
+extern "C" int ref_inference(int n, const float* pos, const float* scl, const float* quat, const float* dens,
+                             const float* rgb, const float* aabb, const float* scene_box, const float* cam,
+                             int W, int H, int white_bg, int max_prim_slice, const int* ids, int n_ids,
+                             float* out_colors, int* out_counts) {
+    params.rnd_sample = 0u;
+    params.max_prim_slice = (unsigned)max_prim_slice;
+    params.bbox_min = make_float3(scene_box[0], scene_box[1], scene_box[2]);
+    params.bbox_max = make_float3(scene_box[3], scene_box[4], scene_box[5]);
+    params.image_width = (unsigned)W;
+    params.image_height = (unsigned)H;
+    params.cam_eye = make_float3(cam[0], cam[1], cam[2]);
+    params.cam_u = make_float3(cam[3], cam[4], cam[5]);
+    params.cam_v = make_float3(cam[6], cam[7], cam[8]);
+    params.cam_w = make_float3(cam[9], cam[10], cam[11]);
+    params.cam_tan_half_fovx = cam[12];
+    params.cam_tan_half_fovy = cam[13];
+    params.densities = const_cast<float*>(dens);
+    params.color_features = const_cast<float*>(rgb);
+    params.positions = (float3*)pos;
+    params.scales = (float3*)scl;
+    params.quaternions = (float4*)quat;
+    /* the program writes colours and adds counts at launch indices: full-size buffers */
+    float* colors = (float*)std::calloc((size_t)W * H * 3, sizeof(float));
+    int* counts = (int*)std::calloc((size_t)W * H, sizeof(int));
+    if (!colors || !counts) { std::free(colors); std::free(counts); return -1; }
+    params.ray_colors = (float3*)colors;
+    params.number_of_gaussians_per_ray = counts;
+    params.number_of_gaussians_per_slab = nullptr;
+    params.handle = 0;
+    params.white_background = (unsigned)white_bg;
+    g_sbt.positions = (float3*)pos; g_sbt.scales = (float3*)scl; g_sbt.quaternions = (float4*)quat;
+    rg_emul_scene.aabb = aabb; rg_emul_scene.n = n; rg_emul_scene.sbt_data = &g_sbt;
+    const int n_rays = ids ? n_ids : W * H;
+#pragma omp parallel for schedule(dynamic, 8)
+    for (int r = 0; r < n_rays; ++r) {
+        rg_emul.launch_idx = make_uint3((unsigned)(ids ? ids[r] : r), 0u, 0u);
+        rg_emul.launch_dim = make_uint3((unsigned)(W * H), 1u, 1u);
+        rg_emul.have_cands = false;
+        __raygen__rg();
+    }
+    for (int r = 0; r < n_rays; ++r) {
+        const int k = ids ? ids[r] : r;
+        for (int c = 0; c < 3; ++c) out_colors[3 * r + c] = colors[3 * k + c];
+        out_counts[r] = counts[k];
+    }
+    std::free(colors);
+    std::free(counts);
     return 0;
 }
 #elif REF_STAGE == 3

@@ -1,6 +1,7 @@
 /*
- * Host-side emulation of the OptiX 7 device API calls that the reference's training programs
- * make (optix_raycasting/cuda_train/{forward,backward}/gaussians_aabb.cu) — TEST
+ * Host-side emulation of the OptiX 7 device API calls that the reference's programs make
+ * (optix_raycasting/cuda_train/{forward,backward}/gaussians_aabb.cu and the inference programs
+ * optix_raycasting/cuda_test/gaussians_aabb.cu) — TEST
  * INFRASTRUCTURE ONLY.  It lets oracle/ref_harness.cpp compile those programs, unmodified,
  * as plain C++ on the CPU so that their own intersection, any-hit, sampling, compositing and
  * adjoint code produce reference outputs for small scenes.
@@ -16,6 +17,7 @@
 #include <cmath>
 #include <vector>
 #include <cstdio>
+#include <cstring>
 
 typedef unsigned long long OptixTraversableHandle;
 typedef unsigned int OptixVisibilityMask;
@@ -28,6 +30,8 @@ struct RgEmulRay {
     uint3 launch_idx;
     uint3 launch_dim;
     unsigned payload0;
+    unsigned payload1, payload2;
+    unsigned attr[6];
     unsigned prim;
     float3 o, d;
     float tmin, tmax;
@@ -60,6 +64,25 @@ static inline bool optixReportIntersection(float t, unsigned /*kind*/) {
     if (t >= rg_emul.tmin && t <= rg_emul.tmax) { rg_emul.reported = true; return true; }
     return false;
 }
+/* report with six 32-bit attributes (read back by the any-hit program) */
+static inline bool optixReportIntersection(float t, unsigned kind, unsigned a0, unsigned a1, unsigned a2,
+                                           unsigned a3, unsigned a4, unsigned a5) {
+    rg_emul.attr[0] = a0; rg_emul.attr[1] = a1; rg_emul.attr[2] = a2;
+    rg_emul.attr[3] = a3; rg_emul.attr[4] = a4; rg_emul.attr[5] = a5;
+    return optixReportIntersection(t, kind);
+}
+static inline unsigned optixGetAttribute_0() { return rg_emul.attr[0]; }
+static inline unsigned optixGetAttribute_1() { return rg_emul.attr[1]; }
+static inline unsigned optixGetAttribute_2() { return rg_emul.attr[2]; }
+static inline unsigned optixGetAttribute_3() { return rg_emul.attr[3]; }
+static inline unsigned optixGetAttribute_4() { return rg_emul.attr[4]; }
+static inline unsigned optixGetAttribute_5() { return rg_emul.attr[5]; }
+static inline unsigned optixGetPayload_1() { return rg_emul.payload1; }
+static inline unsigned optixGetPayload_2() { return rg_emul.payload2; }
+#ifndef __CUDACC__
+static inline unsigned __float_as_uint(float f) { unsigned u; std::memcpy(&u, &f, sizeof u); return u; }
+static inline float __uint_as_float(unsigned u) { float f; std::memcpy(&f, &u, sizeof f); return f; }
+#endif
 static inline void optixTerminateRay() { rg_emul.terminated = true; }
 static inline void optixIgnoreIntersection() {}
 
@@ -102,6 +125,15 @@ static inline void optixTrace(OptixTraversableHandle, float3 o, float3 d, float 
         }
     }
     p0 = rg_emul.payload0;
+}
+
+/* three-payload form (payloads 1 and 2 carry a pointer to the caller's sample buffer) */
+static inline void optixTrace(OptixTraversableHandle h, float3 o, float3 d, float tmin, float tmax, float rt,
+                              OptixVisibilityMask m, unsigned f, unsigned a, unsigned b, unsigned c, unsigned& p0,
+                              unsigned& p1, unsigned& p2) {
+    rg_emul.payload1 = p1;
+    rg_emul.payload2 = p2;
+    optixTrace(h, o, d, tmin, tmax, rt, m, f, a, b, c, p0);
 }
 
 /* device atomics used by the programs, made thread-safe for the OpenMP ray loop */

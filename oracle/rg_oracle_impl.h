@@ -17,6 +17,8 @@
  *                       (computeBufferForward), :500-519 (colorBlending), :521-612
  *                       (__raygen__rg), :621-641 (__anyhit__ah cap semantics)
  *   orc_render_backward optix_raycasting/cuda_train/backward/gaussians_aabb.cu:505-775
+ *   orc_render_inference optix_raycasting/cuda_test/gaussians_aabb.cu:236-470 (inference
+ *                       programs launched by optix_utils.py:302-373)
  * Reference quirks reproduced on request: the sign-dependent root order of the ellipsoid test
  * (camera inside, centre behind: never hit) is always reproduced; the SH degree-3 y-derivative
  * of basis 9 is reproduced when ref_quirks=1.
@@ -523,6 +525,105 @@ int ORC_FN(orc_render_forward)(int n, const REAL* pos, const REAL* scl, const RE
         free(hits);
     }
     if (stats) { stats[0] = st0; stats[1] = st1; stats[2] = st2; }
+    return 0;
+}
+
+/* Inference render (optix_raycasting/cuda_test/gaussians_aabb.cu:236-470, launched by
+ * optix_utils.py:302-373).  Differs from the training forward in three ways:
+ *  - the slab query is [tb, tb + 0.02] without the box-exit clip (:408-409);
+ *  - the samples of a hit step through the conic space from the slab start: m_0 is the scaled
+ *    conic applied to (o + tb d - mu) times sqrt(log(ratio^2)), m_{i+1} = m_i + dt M d (:282-295,
+ *    :501-515), weight_density = exp(-|m|^2 / 2) * density and colour * weight_density;
+ *  - counts[ray] sums the per-slab hit counts (capped at max_prim_slice like the any-hit, :438).
+ * No jitter and no random sample offsets.  Colours, background and blending as the training
+ * forward. */
+static void ORC_FN(slab_buffers_inf)(const SCENE* S, const int* hits, int nh, REAL tb, V3 o, V3 d, REAL* sig,
+                                     V3* C) {
+    for (int i = 0; i < ORC_BUF; ++i) { sig[i] = 0; C[i] = MK(0, 0, 0); }
+    for (int h = 0; h < nh; ++h) {
+        const int g = hits[h];
+        V3 mu = MK(S->pos[3 * g], S->pos[3 * g + 1], S->pos[3 * g + 2]);
+        V3 s = MK(S->scl[3 * g], S->scl[3 * g + 1], S->scl[3 * g + 2]);
+        REAL dens = S->dens[g];
+        REAL ratio = dens / (REAL)0.1;
+        REAL kf = RSQRT(RLOG(ratio * ratio));
+        s = SCL(s, kf);
+        V3 inv = MK((REAL)1 / s.x, (REAL)1 / s.y, (REAL)1 / s.z);
+        V3 M1, M2, M3;
+        ORC_FN(conic_rows)(S->quat + 4 * g, inv, &M1, &M2, &M3);
+        V3 hit = ADD(o, SCL(d, tb));
+        V3 m = SCL(ORC_FN(apply)(M1, M2, M3, SUB(hit, mu)), kf);
+        V3 mdt = SCL(SCL(ORC_FN(apply)(M1, M2, M3, d), kf), ORC_DT);
+        V3 col = MK(S->rgb[3 * g], S->rgb[3 * g + 1], S->rgb[3 * g + 2]);
+        for (int i = 0; i < ORC_BUF; ++i) {
+            REAL wd = REXP((REAL)-0.5f * DOT(m, m)) * dens;
+            if (wd > ORC_STHR) {
+                sig[i] += wd;
+                C[i] = ADD(C[i], SCL(col, wd));
+            }
+            m = ADD(m, mdt);
+        }
+    }
+}
+
+int ORC_FN(orc_render_inference)(int n, const REAL* pos, const REAL* scl, const REAL* quat, const REAL* dens,
+                                 const REAL* rgb, const REAL* aabb, const REAL* scene_box, const REAL* cam,
+                                 int W, int H, int white_bg, int max_prim_slice, const int* ray_ids, int n_rays,
+                                 const int* order, REAL* out, int* counts, long long* stats) {
+    SCENE S = {pos, scl, quat, dens, rgb, n};
+    long long st0 = 0, st1 = 0;
+    int cap = max_prim_slice > 0 ? max_prim_slice : 1024;
+#pragma omp parallel reduction(+ : st0, st1)
+    {
+        CAND* cands = (CAND*)malloc(sizeof(CAND) * (size_t)(n > 0 ? n : 1));
+        int* hits = (int*)malloc(sizeof(int) * (size_t)(n > 0 ? n : 1));
+#pragma omp for schedule(dynamic, 16)
+        for (int rr = 0; rr < n_rays; ++rr) {
+            unsigned idx = ray_ids ? (unsigned)ray_ids[rr] : (unsigned)rr;
+            unsigned seed = 0;
+            V3 o, d;
+            ORC_FN(make_ray)(cam, W, H, idx, 0, &seed, &o, &d);
+            REAL tenter, texit;
+            ORC_FN(scene_clip)(scene_box, o, d, &tenter, &texit);
+            REAL bg = white_bg ? (REAL)1 : (REAL)0;
+            REAL T = 1;
+            V3 col = MK(0, 0, 0);
+            int cnt = 0;
+            if (tenter < texit) {
+                const REAL slab = ORC_DT * (REAL)ORC_BUF;
+                /* candidates over the whole marched range: the last slab reaches past texit */
+                int nc = ORC_FN(gather_cands)(&S, aabb, o, d, tenter, texit + slab, order, cands);
+                REAL tb = tenter;
+                while (tb < texit && T > ORC_TEPS) {
+                    REAL lo = tb, hi = tb + slab;
+                    if (hi > tenter) {
+                        int nh = ORC_FN(slab_hits)(cands, nc, lo, hi, cap, hits, &st0);
+                        if (nh > 0) {
+                            st1 += nh;
+                            cnt += nh;
+                            REAL sig[ORC_BUF]; V3 C[ORC_BUF];
+                            ORC_FN(slab_buffers_inf)(&S, hits, nh, tb, o, d, sig, C);
+                            for (int i = 0; i < ORC_BUF; ++i) {
+                                REAL alpha = (REAL)1 - REXP(-sig[i] * ORC_DT);
+                                V3 c = C[i];
+                                if (sig[i] > 0) c = DIVS(c, sig[i]);
+                                col = ADD(col, SCL(c, T * alpha));
+                                T *= (REAL)1 - alpha;
+                            }
+                        }
+                    }
+                    tb += slab;
+                }
+            }
+            out[3 * rr + 0] = col.x + T * bg;
+            out[3 * rr + 1] = col.y + T * bg;
+            out[3 * rr + 2] = col.z + T * bg;
+            if (counts) counts[rr] = cnt;
+        }
+        free(cands);
+        free(hits);
+    }
+    if (stats) { stats[0] = st0; stats[1] = st1; }
     return 0;
 }
 

@@ -10,7 +10,9 @@ if ROOT not in sys.path:
     sys.path.insert(0, ROOT)
 GOLDEN = os.path.join(ROOT, "tests", "golden")
 SCENES = sorted(os.path.basename(p)[:-4] for p in glob.glob(os.path.join(GOLDEN, "*.npz"))
-                if not p.endswith("sh_twin.npz"))
+                if not p.endswith("sh_twin.npz") and not os.path.basename(p).startswith("infer_"))
+# inference-program fixtures (image + Gaussians per ray)
+INFER_SCENES = sorted(os.path.basename(p)[:-4] for p in glob.glob(os.path.join(GOLDEN, "infer_*.npz")))
 
 
 def pytest_configure(config):

@@ -1,10 +1,11 @@
 """Generate the golden fixtures in tests/golden/ from the reference's own code.
 
 Run in a container where the reference tree is mounted at /root/reference:
-    python tests/golden/make_golden.py
+    python tests/golden/make_golden.py                     (all fixtures)
+    python tests/golden/make_golden.py --inference-only    (the infer_*.npz fixtures only)
 It (1) builds oracle/_ref/ — the reference's training device programs
-(optix_raycasting/cuda_train/{forward,backward}/gaussians_aabb.cu) and SH kernels
-(utils/sh_utils.cu) compiled for the CPU with oracle/ref_shim/optix.h standing in for OptiX — and
+(optix_raycasting/cuda_train/{forward,backward}/gaussians_aabb.cu), its inference programs
+(optix_raycasting/cuda_test/gaussians_aabb.cu) and SH kernels (utils/sh_utils.cu) compiled for the CPU with oracle/ref_shim/optix.h standing in for OptiX — and
 (2) imports the reference's torch SH twin (utils/sh_utils.py: eval_sh, backward_sh).  The fixtures
 hold seeded inputs and those reference outputs; the tests compare the C oracle and the CUDA engine
 against them without needing the reference tree.
@@ -58,6 +59,40 @@ def scene_case(name, P, cam, W, H, white=True, max_prim_slice=1024, jitter=0, rn
     out.update({"in_" + k: v for k, v in P.items()})
     np.savez_compressed(os.path.join(HERE, name + ".npz"), **out)
     print(name, "image mean %.4f" % img.mean(), "overflow", ovf)
+
+
+def inference_case(name, P, cam, W, H, white=True, max_prim_slice=1024):
+    """The reference's inference programs (optix_raycasting/cuda_test/gaussians_aabb.cu): image and
+    Gaussians per ray."""
+    f = np.float32
+    P = {k: np.asarray(v, f) for k, v in P.items()}
+    cv = cam_vec_of(cam).astype(f)
+    nsg = P["sph_gauss_features"].shape[2]
+    sg = P["sph_gauss_features"] if nsg else None
+    kap = P["bandwidth_sharpness"] if nsg else None
+    ax = P["lobe_axis"] if nsg else None
+    rgb = O.ref_forward_sh(cv[:3], P["positions"], P["color_features"], sg, kap, ax)
+    img, counts = O.ref_render_inference(P["positions"], P["scales"], P["quaternions"], P["densities"], rgb, cv, W,
+                                         H, white, max_prim_slice)
+    out = dict(cam=cv, width=np.int32(W), height=np.int32(H), white=np.int32(white),
+               max_prim_slice=np.int32(max_prim_slice), ref_rgb=rgb, ref_image=img, ref_counts=counts)
+    out.update({"in_" + k: v for k, v in P.items()})
+    np.savez_compressed(os.path.join(HERE, name + ".npz"), **out)
+    print(name, "image mean %.4f" % img.mean(), "Gaussians per ray %.1f" % counts.mean())
+
+
+def inference_cases():
+    P = S.small_object(600, seed=1)
+    P["scales"] = P["scales"] * 4.0
+    inference_case("infer_small_object_sh3", P, S.sphere_camera(3.0, 32, 32, 40.0, 1), 32, 32, white=True)
+    P = S.bounded_object(500, seed=2)
+    P["scales"] = P["scales"] * 6.0
+    inference_case("infer_shells_sg8", P, S.sphere_camera(4.0, 28, 24, 40.0, 2), 28, 24, white=False)
+    # a per-slab cap the scene exceeds: the reference keeps the first hits of its traversal, so only
+    # the oracle (same cap semantics) is compared against this one
+    P = S.small_object(600, seed=8)
+    P["scales"] = P["scales"] * 6.0
+    inference_case("infer_capped", P, S.sphere_camera(3.0, 16, 16, 40.0, 8), 16, 16, white=True, max_prim_slice=4)
 
 
 def inside_camera_scene(seed=5):
@@ -115,6 +150,9 @@ def sh_twin_case():
 
 def main():
     subprocess.run(["make", "-s", "-C", os.path.join(REPO, "oracle"), "all", "ref"], check=True)
+    if "--inference-only" in sys.argv:
+        inference_cases()
+        return
     # 1. the small-object distribution (configs' 10k case, thinned) with SH degree 3
     P = S.small_object(600, seed=1)
     P["scales"] = P["scales"] * 4.0
@@ -137,6 +175,7 @@ def main():
     P["color_features"] = P["color_features"][:, :, :4]
     scene_case("midpoint_sh1", P, S.sphere_camera(3.0, 20, 16, 40.0, 6), 20, 16, white=True, rnd_sample=2, seed=6)
     sh_twin_case()
+    inference_cases()
 
 
 if __name__ == "__main__":
