@@ -25,6 +25,9 @@
  *                       (compute_cupy_sh_grad) and the gradient assembly of render_optix.py:170-190
  *   rg_render_forward   RenderOptixFunction.forward, optix_raycasting/render_optix.py:92-132
  *   rg_render_backward  RenderOptixFunction.backward, optix_raycasting/render_optix.py:136-190
+ *   rg_launch_inference optix_raycasting/optix_utils.py:302-373 (launch_pipeline_test) and the
+ *                       programs of cuda_test/gaussians_aabb.cu:236-470
+ *   rg_render_inference the inference render of scripts/test.py:42-132 (bbox, GAS, colour, launch)
  */
 #ifndef RAYGAUSS_B200_H
 #define RAYGAUSS_B200_H
@@ -184,6 +187,18 @@ RG_API int rg_forward_sh(rg_engine* e, const rg_gaussians* g, const rg_camera* c
  * views' rays packed in order, ray y*W+x within a view; final_T (R,) optional. */
 RG_API int rg_launch_forward(rg_engine* e, const rg_camera* cams, int32_t n_cams, const rg_settings* s,
                       float* ray_colors, float* final_T, void* stream);
+/* optix_utils.py:302-373 (launch_pipeline_test) with the inference programs of
+ * optix_raycasting/cuda_test/gaussians_aabb.cu:236-470: a forward render without jitter or random
+ * sample offsets whose slab query is not clipped at the scene-box exit and whose samples step
+ * through the conic space (parity arithmetic).  gaussians_per_ray (R,) int32 is optional: the
+ * per-slab hit counts summed over the ray, each capped at max_prim_slice (exact in the parity
+ * arithmetic; the fast arithmetic counts every list entry whose chunk interval covers the lane). */
+RG_API int rg_launch_inference(rg_engine* e, const rg_camera* cams, int32_t n_cams, const rg_settings* s,
+                        float* ray_colors, int32_t* gaussians_per_ray, void* stream);
+/* bbox -> BVH build (or refit) -> colour -> rg_launch_inference, as rg_render_forward. */
+RG_API int rg_render_inference(rg_engine* e, const rg_gaussians* g, const rg_camera* cams, int32_t n_cams,
+                        const rg_settings* s, int32_t refit, float* ray_colors, int32_t* gaussians_per_ray,
+                        float* rgb_out, void* stream);
 /* optix_utils.py:213-299: recompute the forward's slabs and scatter per-Gaussian gradients into
  * the engine's accumulators (zeroed by this call).  ray_colors are the forward outputs.  When no
  * bbox/BVH/colour/tuning call came after the last rg_launch_forward and cams, n_cams and *s are

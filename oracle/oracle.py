@@ -184,9 +184,9 @@ def render_backward(pos, scl, quat, dens, rgb, cam_vec, width, height, ray_color
 
 
 def render_inference(pos, scl, quat, dens, rgb, cam_vec, width, height, white_bg=True, max_prim_slice=1024,
-                     ray_ids=None, aabb=None, scene_box=None, prec="f32", order=None):
+                     ray_ids=None, aabb=None, scene_box=None, prec="f32", order=None, count_cap=0):
     """Inference render (the reference's cuda_test programs): image (n_rays, 3) and Gaussians per
-    ray (n_rays,) int32."""
+    ray (n_rays,) int32.  ``count_cap`` > 0 caps the per-slab counts without dropping hits."""
     dt = _dt(prec)
     pos, scl, quat, dens, rgb = (_c(a, dt) for a in (pos, scl, quat, dens, rgb))
     if aabb is None or scene_box is None:
@@ -201,7 +201,8 @@ def render_inference(pos, scl, quat, dens, rgb, cam_vec, width, height, white_bg
     getattr(_lib(), "orc_render_inference_" + prec)(
         ctypes.c_int(pos.shape[0]), _p(pos), _p(scl), _p(quat), _p(dens), _p(rgb), _p(aabb), _p(scene_box),
         _p(cam), ctypes.c_int(width), ctypes.c_int(height), ctypes.c_int(int(bool(white_bg))),
-        ctypes.c_int(max_prim_slice), _p(ids), ctypes.c_int(nr), _p(order), _p(out), _p(counts), _p(stats))
+        ctypes.c_int(max_prim_slice), ctypes.c_int(count_cap), _p(ids), ctypes.c_int(nr), _p(order), _p(out),
+        _p(counts), _p(stats))
     return out, counts
 
 

@@ -534,7 +534,8 @@ int ORC_FN(orc_render_forward)(int n, const REAL* pos, const REAL* scl, const RE
  *  - the samples of a hit step through the conic space from the slab start: m_0 is the scaled
  *    conic applied to (o + tb d - mu) times sqrt(log(ratio^2)), m_{i+1} = m_i + dt M d (:282-295,
  *    :501-515), weight_density = exp(-|m|^2 / 2) * density and colour * weight_density;
- *  - counts[ray] sums the per-slab hit counts (capped at max_prim_slice like the any-hit, :438).
+ *  - counts[ray] sums the per-slab hit counts (capped at max_prim_slice like the any-hit, :438;
+ *    count_cap > 0 caps the counts alone, for an engine that keeps every hit but counts the same).
  * No jitter and no random sample offsets.  Colours, background and blending as the training
  * forward. */
 static void ORC_FN(slab_buffers_inf)(const SCENE* S, const int* hits, int nh, REAL tb, V3 o, V3 d, REAL* sig,
@@ -568,11 +569,12 @@ static void ORC_FN(slab_buffers_inf)(const SCENE* S, const int* hits, int nh, RE
 
 int ORC_FN(orc_render_inference)(int n, const REAL* pos, const REAL* scl, const REAL* quat, const REAL* dens,
                                  const REAL* rgb, const REAL* aabb, const REAL* scene_box, const REAL* cam,
-                                 int W, int H, int white_bg, int max_prim_slice, const int* ray_ids, int n_rays,
-                                 const int* order, REAL* out, int* counts, long long* stats) {
+                                 int W, int H, int white_bg, int max_prim_slice, int count_cap, const int* ray_ids,
+                                 int n_rays, const int* order, REAL* out, int* counts, long long* stats) {
     SCENE S = {pos, scl, quat, dens, rgb, n};
     long long st0 = 0, st1 = 0;
     int cap = max_prim_slice > 0 ? max_prim_slice : 1024;
+    int ccap = count_cap > 0 ? count_cap : cap;   /* per-slab cap of the counts alone (0: the hit cap) */
 #pragma omp parallel reduction(+ : st0, st1)
     {
         CAND* cands = (CAND*)malloc(sizeof(CAND) * (size_t)(n > 0 ? n : 1));
@@ -600,7 +602,7 @@ int ORC_FN(orc_render_inference)(int n, const REAL* pos, const REAL* scl, const 
                         int nh = ORC_FN(slab_hits)(cands, nc, lo, hi, cap, hits, &st0);
                         if (nh > 0) {
                             st1 += nh;
-                            cnt += nh;
+                            cnt += nh < ccap ? nh : ccap;
                             REAL sig[ORC_BUF]; V3 C[ORC_BUF];
                             ORC_FN(slab_buffers_inf)(&S, hits, nh, tb, o, d, sig, C);
                             for (int i = 0; i < ORC_BUF; ++i) {

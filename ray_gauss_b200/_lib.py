@@ -87,6 +87,9 @@ SIGNATURES = {
     "rg_forward_sh": (ctypes.c_int, [_P, ctypes.POINTER(rg_gaussians), _P, ctypes.c_int32, _P, _P]),
     "rg_launch_forward": (ctypes.c_int, [_P, _P, ctypes.c_int32, ctypes.POINTER(rg_settings), _P, _P, _P]),
     "rg_launch_backward": (ctypes.c_int, [_P, _P, ctypes.c_int32, ctypes.POINTER(rg_settings), _P, _P, _P]),
+    "rg_launch_inference": (ctypes.c_int, [_P, _P, ctypes.c_int32, ctypes.POINTER(rg_settings), _P, _P, _P]),
+    "rg_render_inference": (ctypes.c_int, [_P, ctypes.POINTER(rg_gaussians), _P, ctypes.c_int32,
+                                           ctypes.POINTER(rg_settings), ctypes.c_int32, _P, _P, _P, _P]),
     "rg_backward_sh": (ctypes.c_int, [_P, ctypes.POINTER(rg_gaussians), _P, ctypes.c_int32,
                                       ctypes.POINTER(rg_settings), ctypes.POINTER(rg_gradients), _P]),
     "rg_render_forward": (ctypes.c_int, [_P, ctypes.POINTER(rg_gaussians), _P, ctypes.c_int32,

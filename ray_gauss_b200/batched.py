@@ -111,3 +111,19 @@ def render_views(params: dict, views: BatchedViews):
                                        params["densities"], params["color_features"],
                                        params.get("sph_gauss_features"), params.get("bandwidth_sharpness"),
                                        params.get("lobe_axis"), views)
+
+
+def render_views_inference(params: dict, views: BatchedViews, counts: bool = False):
+    """Inference render of every view of ``views`` in one launch (the reference's cuda_test
+    programs: no jitter or random sample offsets, slab queries not clipped at the scene-box exit).
+    Returns packed ray colours and, with ``counts``, the Gaussians per ray (int32)."""
+    eng = views.engine or engine_for(params["positions"].device)
+    nsg = 0 if params.get("sph_gauss_features") is None else params["sph_gauss_features"].shape[2]
+    g = make_gaussians(params["positions"], params["scales"], params["quaternions"], params["densities"],
+                       params["color_features"], params.get("sph_gauss_features") if nsg else None,
+                       params.get("bandwidth_sharpness") if nsg else None, params.get("lobe_axis") if nsg else None)
+    cams_t, _, _ = eng.cameras(views.cameras, views.supersampling)
+    with torch.no_grad():
+        out, cnt = eng.render_inference(g, cams_t, len(views.cameras), views.n_rays, _st(views), refit=views.update,
+                                        counts=counts)
+    return (out, cnt) if counts else out

@@ -71,7 +71,7 @@ __global__ void __launch_bounds__(256) k_prepass(long long n, const float* __res
         float jx = __fdiv_rn(1.f, MUL(sx, dl_is)), jy = __fdiv_rn(1.f, MUL(sy, dl_is)),
               jz = __fdiv_rn(1.f, MUL(sz, dl_is));
         LeafIS is;
-        is.u = make_float4(MUL(R00, jx), MUL(R10, jx), MUL(R20, jx), 0.f);
+        is.u = make_float4(MUL(R00, jx), MUL(R10, jx), MUL(R20, jx), dl_is);   // .w: inference conic scale
         is.v = make_float4(MUL(R01, jy), MUL(R11, jy), MUL(R21, jy), 0.f);
         is.w = make_float4(MUL(R02, jz), MUL(R12, jz), MUL(R22, jz), 0.f);
 #undef MUL

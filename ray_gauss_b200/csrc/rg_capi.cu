@@ -394,6 +394,41 @@ int rg_launch_forward(rg_engine* e, const rg_camera* cams, int32_t n_cams, const
     return RG_OK;
 }
 
+int rg_launch_inference(rg_engine* e, const rg_camera* cams, int32_t n_cams, const rg_settings* s,
+                        float* ray_colors, int32_t* gaussians_per_ray, void* stream) {
+    if (!e || !s || !ray_colors) return RG_ERR_INVALID_ARG;
+    int rc = check_views(cams, n_cams);
+    if (rc) return rc;
+    if (e->n_built <= 0 || e->colors_views < n_cams) return RG_ERR_STATE;
+    if ((rc = set_device(e))) return rc;
+    // the inference programs sample without jitter or random offsets
+    rg_settings si = *s;
+    si.jitter = 0;
+    si.rnd_sample = 0;
+    RG_CUDA(rg::launch_setup_views(cams, n_cams, e->vt, e->work_counter, S(stream)), "setup views");
+    rg::RenderArgs a;
+    fill_args(e, cams, &si, a);
+    a.ray_colors = ray_colors;
+    a.infer = 1;
+    a.counts = gaussians_per_ray;
+    int grid = render_grid(e, false, kernel_mode(&si));
+    RG_CUDA(rg::launch_render(false, si.mode, e->tuning.list_capacity, grid, a, S(stream)), "render inference");
+    e->launches += 2;
+    return RG_OK;
+}
+
+int rg_render_inference(rg_engine* e, const rg_gaussians* g, const rg_camera* cams, int32_t n_cams,
+                        const rg_settings* s, int32_t refit, float* ray_colors, int32_t* gaussians_per_ray,
+                        float* rgb_out, void* stream) {
+    int rc = rg_ellipsoids_bbox(e, g, nullptr, nullptr, stream);
+    if (rc) return rc;
+    if (refit && e->n_built == g->n) rc = rg_bvh_refit(e, stream);
+    else rc = rg_bvh_build(e, stream);
+    if (rc) return rc;
+    if ((rc = rg_forward_sh(e, g, cams, n_cams, rgb_out, stream))) return rc;
+    return rg_launch_inference(e, cams, n_cams, s, ray_colors, gaussians_per_ray, stream);
+}
+
 int rg_launch_backward(rg_engine* e, const rg_camera* cams, int32_t n_cams, const rg_settings* s,
                        const float* ray_colors, const float* dloss_dray_colors, void* stream) {
     if (!e || !s || !ray_colors || !dloss_dray_colors) return RG_ERR_INVALID_ARG;

@@ -128,7 +128,8 @@ struct __align__(16) LeafRec {
 
 // Threshold-ellipsoid conic of a leaf in the reference's arithmetic, 48 bytes: the rotation columns
 // scaled by 1/(s_j sqrt(log((density/0.1)^2))) (forward/gaussians_aabb.cu:341-357), used by the
-// exact ray/ellipsoid interval test of the parity arithmetic.
+// exact ray/ellipsoid interval test of the parity arithmetic; u.w holds sqrt(log((density/0.1)^2)),
+// the factor the inference programs scale their sample conic back with.
 struct __align__(16) LeafIS {
     float4 u, v, w;
 };

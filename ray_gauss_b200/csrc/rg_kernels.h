@@ -58,6 +58,10 @@ struct RenderArgs {
     unsigned* rec_tile;           // first chunk record of each tile (kNoRecord: none)
     int rec_tiles;                // entries of rec_tile
     int replay;                   // backward: replay the records
+    // inference launch (the reference's cuda_test programs): slab query without the box-exit clip,
+    // conic-space sample stepping (parity arithmetic), optional Gaussians per ray
+    int infer;
+    int* counts;
 };
 
 cudaError_t launch_prepass(const rg_gaussians* g, GaussRec* rec, float* aabb, int* scene_ord, DevStatus* st,

@@ -232,8 +232,8 @@ __device__ __noinline__ bool slab_k_hit(float tb, float tenter, float texit, int
 // slab at each end: the parity arithmetic settles the ends exactly here, the fast arithmetic
 // evaluates them (their samples fall outside the threshold ellipsoid).
 template <bool FAST>
-__device__ __forceinline__ void slab_range(const RayState& r, int K, int nv, float seg_hi, float root1, float root2,
-                                           int& lo, int& hi) {
+__device__ __forceinline__ void slab_range(const RayState& r, int K, int nv, float seg_hi, float tclip, float root1,
+                                           float root2, int& lo, int& hi) {
     lo = 255;
     hi = -1;
     if (K <= kExactChunk) {
@@ -243,7 +243,7 @@ __device__ __forceinline__ void slab_range(const RayState& r, int K, int nv, flo
         for (int kk = 0; kk < kExactChunk; ++kk) {
             if (kk < nv) {
                 float tn = t + kSlab;
-                float th = fminf(r.texit, tn);
+                float th = fminf(tclip, tn);
                 if (th > r.tenter && fmaxf(t, root1) <= fminf(th, root2)) {
                     lo = min(lo, kk);
                     hi = kk;
@@ -263,15 +263,15 @@ __device__ __forceinline__ void slab_range(const RayState& r, int K, int nv, flo
             // Parity: settle both ends exactly.  A slab whose hit or miss the margins cannot decide
             // gets the reference's per-slab test (rare: its interval end lies within the margin
             // of a slab edge or of the box exit).
-            const float e = fminf((r.texit - r.tb) * kInvSlab, 4096.f);
+            const float e = fminf((tclip - r.tb) * kInvSlab, 4096.f);
             while (lo <= hi) {
                 const int c = classify_slab(lo, a, b, e, m);
-                if (c > 0 || (c == 0 && slab_k_hit(r.tb, r.tenter, r.texit, lo, root1, root2))) break;
+                if (c > 0 || (c == 0 && slab_k_hit(r.tb, r.tenter, tclip, lo, root1, root2))) break;
                 ++lo;
             }
             while (hi >= lo) {
                 const int c = classify_slab(hi, a, b, e, m);
-                if (c > 0 || (c == 0 && slab_k_hit(r.tb, r.tenter, r.texit, hi, root1, root2))) break;
+                if (c > 0 || (c == 0 && slab_k_hit(r.tb, r.tenter, tclip, hi, root1, root2))) break;
                 --hi;
             }
         }
@@ -356,7 +356,10 @@ __device__ __forceinline__ bool leaf_entry(WarpSmem<FAST, CAP>& sm, const Render
             float4 m4 = __ldg(reinterpret_cast<const float4*>(a.rec + leaf));
             ok = roots_exact(load_is(a.is_rec, leaf), f3(m4.x, m4.y, m4.z), r, root1, root2);
         }
-        if (ok) slab_range<FAST>(r, K, nv, seg_hi, root1, root2, lo, hi);
+        // the slab query ends at the box exit in training launches and at the slab end in
+        // inference launches (cuda_test/gaussians_aabb.cu:408-409)
+        const float tclip = a.infer ? INFINITY : r.texit;
+        if (ok) slab_range<FAST>(r, K, nv, seg_hi, tclip, root1, root2, lo, hi);
     }
     unsigned any = __ballot_sync(kFull, lo <= hi);
     if (!any) return true;
@@ -589,6 +592,35 @@ __device__ __forceinline__ int slab_buffers(const WarpSmem<FAST, CAP>& sm, int k
                         if (GDOT) gC[i] = fmaf(gcol, dw, gC[i]);
                         else C[i] = C[i] + col * dw;
                     }
+                }
+            } else if (!GDOT && a.infer) {
+                // Inference programs (cuda_test/gaussians_aabb.cu:282-295, :501-515): the samples step
+                // through the scaled conic space from the slab start, m_{i+1} = m_i + dt * M d, and
+                // weight * density multiplies the colour.  Reference operation order.
+                const LeafIS is = load_is(a.is_rec, leaf);
+                const float kf = is.u.w;   // sqrt(log(ratio^2)) of the Gaussian
+                const float3 U = f3(is.u.x, is.u.y, is.u.z), V = f3(is.v.x, is.v.y, is.v.z),
+                             W = f3(is.w.x, is.w.y, is.w.z);
+                const float3 xg = f3(__fsub_rn(__fadd_rn(r.o.x, __fmul_rn(r.tb, r.d.x)), mu.x),
+                                     __fsub_rn(__fadd_rn(r.o.y, __fmul_rn(r.tb, r.d.y)), mu.y),
+                                     __fsub_rn(__fadd_rn(r.o.z, __fmul_rn(r.tb, r.d.z)), mu.z));
+                float3 m = f3(__fmul_rn(dot_rn(U, xg), kf), __fmul_rn(dot_rn(V, xg), kf),
+                              __fmul_rn(dot_rn(W, xg), kf));
+                const float3 mdt = f3(__fmul_rn(__fmul_rn(dot_rn(U, r.d), kf), kDt),
+                                      __fmul_rn(__fmul_rn(dot_rn(V, r.d), kf), kDt),
+                                      __fmul_rn(__fmul_rn(dot_rn(W, r.d), kf), kDt));
+#pragma unroll
+                for (int i = 0; i < kBuf; ++i) {
+                    const float power = __fmul_rn(-0.5f, dot_rn(m, m));
+                    float w = expf(power);
+                    float wd = __fmul_rn(w, dn);
+                    if (fabsf(wd - kSigThr) < 4e-8f) wd = __fmul_rn((float)exp((double)power), dn);
+                    if (wd > kSigThr) {
+                        sig[i] = __fadd_rn(sig[i], wd);
+                        C[i] = f3(__fadd_rn(C[i].x, __fmul_rn(col4.x, wd)), __fadd_rn(C[i].y, __fmul_rn(col4.y, wd)),
+                                  __fadd_rn(C[i].z, __fmul_rn(col4.z, wd)));
+                    }
+                    m = f3(__fadd_rn(m.x, mdt.x), __fadd_rn(m.y, mdt.y), __fadd_rn(m.z, mdt.z));
                 }
             } else {
 #pragma unroll
@@ -963,6 +995,8 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, min_blocks<BWD, FAST>()) 
 
         int K = min(kExactChunk, kmax);
         int rounds = 0;
+        // end of the searched range: an inference launch queries the last slab in full
+        const float t_end = a.infer ? r.texit + kSlab : r.texit;
         // hit-list record of this tile: the forward appends chunk records, the backward replays them
         const bool rec_here = a.rec_arena != nullptr && tile < a.rec_tiles;
         if (lane == 0) {
@@ -997,10 +1031,10 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, min_blocks<BWD, FAST>()) 
                     for (int kk = 0; kk < K; ++kk) {
                         if (t < r.texit) { nv = kk + 1; t = t + kSlab; } else break;
                     }
-                    seg_hi = fminf(r.texit, t);
+                    seg_hi = fminf(t_end, t);
                 } else {
                     nv = K;
-                    seg_hi = fminf(r.texit, r.tb + (float)(K + 1) * kSlab);
+                    seg_hi = fminf(t_end, r.tb + (float)(K + 1) * kSlab);
                 }
                 // a slab step that no longer changes tb (|t| beyond ~2^19) would march forever
                 if (!(r.tb < r.texit) || r.tb + kSlab == r.tb) { r.alive = false; on = false; nv = 0; }
@@ -1077,7 +1111,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, min_blocks<BWD, FAST>()) 
                                                           nwords(count), lane, ws);
                     if (has) {
                         ++slabs_acc;
-                        hits_acc += nh;
+                        hits_acc += (!BWD && a.counts) ? min(nh, a.max_prim_slice) : nh;
                         if (nh > a.max_prim_slice) atomicAdd(&a.st->slab_cap_exceeded, 1ull);
                     }
                     if (!BWD) {
@@ -1130,7 +1164,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, min_blocks<BWD, FAST>()) 
                 }
                 if (has) {
                     ++slabs_acc;
-                    hits_acc += nh;
+                    hits_acc += (!BWD && a.counts) ? min(nh, a.max_prim_slice) : nh;
                     if (nh > a.max_prim_slice) atomicAdd(&a.st->slab_cap_exceeded, 1ull);
                 }
                 if (!BWD) {
@@ -1171,6 +1205,9 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, min_blocks<BWD, FAST>()) 
             a.ray_colors[3 * ray_g + 1] = __fadd_rn(r.C.y, __fmul_rn(r.T, bg));
             a.ray_colors[3 * ray_g + 2] = __fadd_rn(r.C.z, __fmul_rn(r.T, bg));
             if (a.final_T) a.final_T[ray_g] = r.T;
+            // Gaussians per ray (inference launches): the per-slab hit counts, each capped at
+            // max_prim_slice like the reference any-hit program (cuda_test/gaussians_aabb.cu:438)
+            if (a.counts) a.counts[ray_g] = (int)hits_acc;
         }
     }
     // counters: one atomic per warp and counter

@@ -255,6 +255,29 @@ class Engine:
         self.launch_forward(cams_t, n_cams, settings, ray_colors, fT)
         return ray_colors, fT
 
+    def launch_inference(self, cams_t, n_cams, settings, ray_colors, counts=None):
+        with self._timed("launch_inference"):
+            check(self.lib.rg_launch_inference(self.h, _ptr(cams_t), int(n_cams), ctypes.byref(settings),
+                                               _ptr(ray_colors), _ptr(counts), _stream()), self.h,
+                  "rg_launch_inference")
+
+    def render_inference(self, g: GaussianBatch, cams_t, n_cams, n_rays, settings, refit=False, counts=False):
+        """Inference render (optix_utils.py:302-373 with the cuda_test programs): bbox -> BVH build
+        (or refit) -> colour -> inference launch.  Returns (ray colours (R,3), Gaussians per ray
+        (R,) int32 or None)."""
+        ray_colors = torch.empty((n_rays, 3), dtype=torch.float32, device=self.device)
+        cnt = torch.empty((n_rays,), dtype=torch.int32, device=self.device) if counts else None
+        with self._timed("prepare"):
+            self.ellipsoids_bbox(g)
+            if refit and self._built_n == g.n:
+                self.bvh_refit()
+            else:
+                self.bvh_build()
+                self._built_n = g.n
+            self.forward_sh(g, cams_t, n_cams)
+        self.launch_inference(cams_t, n_cams, settings, ray_colors, cnt)
+        return ray_colors, cnt
+
     def alloc_grads(self, g: GaussianBatch):
         n, dev = g.n, self.device
         f = dict(dtype=torch.float32, device=dev)

@@ -156,9 +156,21 @@ def launch_pipeline_backward(pipeline, sbt, gas, bbox_min, bbox_max, camera, den
 
 
 def launch_pipeline_test(pipeline, sbt, gas, bbox_min, bbox_max, camera, densities, color_features, positions,
-                         scales, quaternions, max_prim_slice, rnd_sample, supersampling, white_background):
-    """Inference render (optix_utils.py:302-373): the forward launch without gradients."""
+                         scales, quaternions, max_prim_slice, rnd_sample, supersampling, white_background,
+                         return_counts=False, mode="parity"):
+    """Inference render (optix_utils.py:302-373 with the cuda_test programs) on per-Gaussian colours
+    ``color_features`` (N,3): no jitter, no random sample offsets (``rnd_sample`` is accepted and
+    ignored, as by those programs), slab queries not clipped at the scene-box exit.  Returns ray
+    colours (R,3); with ``return_counts`` also the Gaussians per ray (R,) int32, which the reference
+    computes but does not return."""
+    eng = gas if isinstance(gas, Engine) else engine_for(positions.device)
+    rgb = color_features.reshape(-1, 3).float()
+    sh0 = ((rgb - 0.5) / 0.28209479177387814).reshape(-1, 3, 1).contiguous()
+    g = make_gaussians(positions, scales, quaternions, densities, sh0)
+    cams_t, recs, _ = eng.cameras([camera], tuple(supersampling))
+    mode_id = {"parity": 0, "fast": 1}[mode]
+    st = settings_struct(white_background, 0, 0, max_prim_slice, 0, mode_id)
     with torch.no_grad():
-        return launch_pipeline_forward(None, None, gas, bbox_min, bbox_max, camera, densities, color_features,
-                                       positions, scales, quaternions, max_prim_slice, 0, 0, rnd_sample,
-                                       supersampling, white_background)
+        out, cnt = eng.render_inference(g, cams_t, 1, recs[0].width * recs[0].height, st, refit=True,
+                                        counts=return_counts)
+    return (out, cnt) if return_counts else out
