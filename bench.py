@@ -330,6 +330,25 @@ def our_arm(args, rank, world, local):
         e2e = {"value": round(world * R / (e_ms * 1e-3) / 1e6, 3), "unit": "Mrays/s", "h2d_bytes_per_step": int(h2d),
                "d2h_bytes_per_step": 4, "ms_per_step": round(e_ms, 3)}
 
+    # ---- inference render (launch_pipeline_test form) of the same views: forward only ----
+    inference = None
+    if not args.no_plain:
+        from ray_gauss_b200.batched import render_views_inference
+        for _ in range(2):
+            render_views_inference(Pb, views)
+        torch.cuda.synchronize()
+        i0 = torch.cuda.Event(enable_timing=True)
+        i1 = torch.cuda.Event(enable_timing=True)
+        isteps = max(2, args.steps)
+        i0.record()
+        for _ in range(isteps):
+            render_views_inference(Pb, views)
+        i1.record()
+        torch.cuda.synchronize()
+        i_ms = i0.elapsed_time(i1) / isteps
+        inference = {"value": round(R / (i_ms * 1e-3) / 1e6, 3), "unit": "Mrays/s", "ms_per_step": round(i_ms, 3),
+                     "form": "render_views_inference: bbox + LBVH + colour + inference launch, BF16, fast arithmetic"}
+
     # ---- plain FP32 single-view drop-in form on the same views ----
     plain = None
     if not args.no_plain:
@@ -392,6 +411,12 @@ def our_arm(args, rank, world, local):
         "counters_per_step": {k: (v if k == "record_words" else v // max(1, args.steps)) for k, v in st.items()},
         "tuning": {k: v for k, v in tuning.items() if k != "ms"},
         "graph_replay": graph,
+        "forward_only": {"value": round(R / (fwd_ms * 1e-3) / 1e6, 3), "unit": "Mrays/s",
+                         "ms_per_launch": round(fwd_ms, 3), "form": "the headline step's forward launch"},
+        "hit_samples": {"value": round(8 * st.get("hit_pairs", 0) / max(1, args.steps) / (ms_max * 1e-3) / 1e9, 3),
+                        "unit": "G hit-samples/s", "form": "8 samples per (ray, slab, Gaussian) pair, forward + "
+                                                          "backward recompute, per step time"},
+        "inference": inference,
         "plain_fp32_single_view": plain,
         "batched_over_plain": round(value / world / plain["value"], 3) if plain else None,
         "accuracy": accuracy,

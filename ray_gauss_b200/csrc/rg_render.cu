@@ -344,7 +344,7 @@ __device__ __forceinline__ void flush_stats(WarpSmem<FAST, CAP>& sm, WarpStats& 
 template <bool FAST, int CAP>
 __device__ __forceinline__ bool leaf_entry(WarpSmem<FAST, CAP>& sm, const RenderArgs& a, const RayState& r, bool on,
                                            float seg_hi, int K, int nv, int leaf, int& count, int lane,
-                                           WarpStats& ws) {
+                                           WarpStats& ws, bool infer) {
     ++ws.leaf_tests;
     int lo = 255, hi = -1;
     if (on) {
@@ -358,7 +358,7 @@ __device__ __forceinline__ bool leaf_entry(WarpSmem<FAST, CAP>& sm, const Render
         }
         // the slab query ends at the box exit in training launches and at the slab end in
         // inference launches (cuda_test/gaussians_aabb.cu:408-409)
-        const float tclip = a.infer ? INFINITY : r.texit;
+        const float tclip = infer ? INFINITY : r.texit;
         if (ok) slab_range<FAST>(r, K, nv, seg_hi, tclip, root1, root2, lo, hi);
     }
     unsigned any = __ballot_sync(kFull, lo <= hi);
@@ -411,7 +411,7 @@ __device__ __forceinline__ void finish_list(WarpSmem<FAST, CAP>& sm, int count, 
 // filled up before the traversal finished.
 template <bool FAST, int CAP>
 __device__ int traverse(WarpSmem<FAST, CAP>& sm, const RenderArgs& a, const RayState& r, bool on, float seg_hi,
-                        int K, int nv, int cursor, bool& ovf, int lane, WarpStats& ws) {
+                        int K, int nv, int cursor, bool& ovf, int lane, WarpStats& ws, bool infer) {
     int count = 0;
     ++ws.traversals;
     ovf = false;
@@ -457,7 +457,7 @@ __device__ int traverse(WarpSmem<FAST, CAP>& sm, const RenderArgs& a, const RayS
             }
         } else {
             int leaf = ~cur;
-            if (leaf > cursor && !leaf_entry<FAST, CAP>(sm, a, r, on, seg_hi, K, nv, leaf, count, lane, ws)) {
+            if (leaf > cursor && !leaf_entry<FAST, CAP>(sm, a, r, on, seg_hi, K, nv, leaf, count, lane, ws, infer)) {
                 ovf = true;
                 break;
             }
@@ -485,7 +485,7 @@ __device__ int replay_list(WarpSmem<FAST, CAP>& sm, const RenderArgs& a, const R
         for (int j = 0; j < m; ++j) {
             const int leaf = __shfl_sync(kFull, mine, j);
             if (leaf >= 0 && leaf < a.n_leaves)
-                leaf_entry<FAST, CAP>(sm, a, r, on, seg_hi, K, nv, leaf, count, lane, ws);
+                leaf_entry<FAST, CAP>(sm, a, r, on, seg_hi, K, nv, leaf, count, lane, ws, false);
         }
     }
     finish_list<FAST, CAP>(sm, count, K, lane, ws);
@@ -996,7 +996,8 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, min_blocks<BWD, FAST>()) 
         int K = min(kExactChunk, kmax);
         int rounds = 0;
         // end of the searched range: an inference launch queries the last slab in full
-        const float t_end = a.infer ? r.texit + kSlab : r.texit;
+        const bool infer = !BWD && a.infer;
+        const float t_end = infer ? r.texit + kSlab : r.texit;
         // hit-list record of this tile: the forward appends chunk records, the backward replays them
         const bool rec_here = a.rec_arena != nullptr && tile < a.rec_tiles;
         if (lane == 0) {
@@ -1047,7 +1048,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, min_blocks<BWD, FAST>()) 
                                                lane, ws);
                 ++ws.replays;
             } else {
-                count = traverse<FAST, CAP>(sm, a, r, on, seg_hi, K, nv, -1, ovf, lane, ws);
+                count = traverse<FAST, CAP>(sm, a, r, on, seg_hi, K, nv, -1, ovf, lane, ws, infer);
             }
             const unsigned long long* occ = sm.occ;
             if (ovf && K > 1) {
@@ -1158,7 +1159,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, min_blocks<BWD, FAST>()) 
                     int cursor = sm.ids[count - 1];
                     __syncwarp();
                     if (lane == 0) atomicAdd(&a.st->list_passes, 1ull);
-                    count = traverse<FAST, CAP>(sm, a, r, on, seg_hi, 1, nv, cursor, more, lane, ws);
+                    count = traverse<FAST, CAP>(sm, a, r, on, seg_hi, 1, nv, cursor, more, lane, ws, infer);
                     nh += slab_buffers<FAST, CAP, BWD>(sm, 0, 1, has, r, a, rgb_base, roff, sig, Cb, gC,
                                                        nwords(count), lane, ws);
                 }
@@ -1179,7 +1180,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, min_blocks<BWD, FAST>()) 
                     int cursor = -1;
                     bool more2 = true;
                     while (more2) {
-                        count = traverse<FAST, CAP>(sm, a, r, on, seg_hi, 1, nv, cursor, more2, lane, ws);
+                        count = traverse<FAST, CAP>(sm, a, r, on, seg_hi, 1, nv, cursor, more2, lane, ws, infer);
                         slab_adjoint<FAST, CAP>(sm, 0, 1, act, r, a, rgb_base, roff, H, F, nwords(count), lane, ws);
                         if (more2) cursor = sm.ids[count - 1];
                         __syncwarp();
