@@ -291,6 +291,54 @@ def our_arm(args, rank, world, local):
         views.update = False
         del gstep, gleaves
 
+    # ---- a whole training iteration on the FP32 trained tensors of the reference's point cloud:
+    #      get_data activations + the graph above + the fused Adam / statistics / clamp tail; and
+    #      that tail alone ----
+    train = None
+    if not args.no_graph:
+        from ray_gauss_b200.graph import GraphedStep
+        from ray_gauss_b200.train_tail import FusedTrainTail, LrSchedule, point_cloud_data, raw_from_render_inputs
+        tleaves = {k: v.detach().contiguous() for k, v in raw_from_render_inputs(P32).items()}
+        tparams = {k: v for k, v in tleaves.items() if v.numel()}
+        tail = FusedTrainTail(tparams, {k: LrSchedule(1e-5) for k in tparams},
+                              roles={"positions": "positions", "densities": "densities", "scales": "scales",
+                                     "quaternions": "quaternions"})
+        min_scale = torch.full((n,), -12.0, device=dev)
+        tstep = GraphedStep(tleaves, views, target, tail=tail, min_scale=min_scale,
+                            activation=lambda r: point_cloud_data(r, normalized_quaternion=False))
+        tstep.replay()
+        torch.cuda.synchronize()
+        g0 = torch.cuda.Event(enable_timing=True)
+        g1 = torch.cuda.Event(enable_timing=True)
+        g0.record()
+        for _ in range(args.steps):
+            tstep.replay()
+        g1.record()
+        torch.cuda.synchronize()
+        t_ms = g0.elapsed_time(g1) / args.steps
+        tgrads = {k: tstep.grads[k].contiguous() for k in tparams}
+        tail.step(min_scale=min_scale, grads=tgrads)
+        torch.cuda.synchronize()
+        g0.record()
+        for _ in range(args.steps):
+            tail.step(min_scale=min_scale, grads=tgrads)
+        g1.record()
+        torch.cuda.synchronize()
+        tail_ms = g0.elapsed_time(g1) / args.steps
+        # param, exp_avg, exp_avg_sq read + written and the gradient read per float; per Gaussian the
+        # three statistics read + written and min_scale read
+        tail_bytes = 28 * sum(v.numel() for v in tparams.values()) + 28 * n
+        tail_gbs = tail_bytes / (tail_ms * 1e-3) / 1e9
+        train = {"value": round(R / (t_ms * 1e-3) / 1e6, 3), "unit": "Mrays/s", "ms_per_step": round(t_ms, 3),
+                 "form": "GraphedStep(tail=FusedTrainTail, activation=point_cloud_data).replay() on the FP32 "
+                         "trained tensors: get_data activations + LBVH refit + colour + forward + MSE + backward + "
+                         "Adam on every tensor + statistics + clamps in one CUDA graph",
+                 "tail": {"kernel": "k_train_tail (rg_train_tail_step)", "ms_per_launch": round(tail_ms, 4),
+                          "algorithmic_bytes_per_launch": int(tail_bytes), "achieved_gbs": round(tail_gbs, 1),
+                          "peak_gbs": peak, "frac": round(tail_gbs / peak, 4), "bound": "hbm"}}
+        views.update = False
+        del tstep, tleaves, tparams, tail, tgrads
+
     # ---- e2e through the public API: host parameters and targets in, loss out ----
     e2e = None
     if rank == 0 or True:
@@ -411,6 +459,7 @@ def our_arm(args, rank, world, local):
         "counters_per_step": {k: (v if k == "record_words" else v // max(1, args.steps)) for k, v in st.items()},
         "tuning": {k: v for k, v in tuning.items() if k != "ms"},
         "graph_replay": graph,
+        "train_step": train,
         "forward_only": {"value": round(R / (fwd_ms * 1e-3) / 1e6, 3), "unit": "Mrays/s",
                          "ms_per_launch": round(fwd_ms, 3), "form": "the headline step's forward launch"},
         "hit_samples": {"value": round(8 * st.get("hit_pairs", 0) / max(1, args.steps) / (ms_max * 1e-3) / 1e9, 3),

@@ -28,6 +28,8 @@
  *   rg_launch_inference optix_raycasting/optix_utils.py:302-373 (launch_pipeline_test) and the
  *                       programs of cuda_test/gaussians_aabb.cu:236-470
  *   rg_render_inference the inference render of scripts/test.py:42-132 (bbox, GAS, colour, launch)
+ *   rg_train_tail_step  the step tail of scripts/train.py:121-181 (statistics, the optimizer
+ *                       managers' Adam steps of classes/optimizer.py:13-21, parameter clamps)
  */
 #ifndef RAYGAUSS_B200_H
 #define RAYGAUSS_B200_H
@@ -243,6 +245,48 @@ RG_API uint64_t rg_kernel_launches(const rg_engine* e);
 RG_API const char* rg_error_string(int code);
 RG_API const char* rg_last_cuda_error(const rg_engine* e);
 RG_API int rg_abi_version(void);
+
+/* ---- Fused training-step tail (scripts/train.py:121-181) ----------------------------------------
+ * One launch over the Gaussians: the densification statistics of the position gradient
+ * (classes/point_cloud.py:633-640), one Adam step on every listed tensor (classes/optimizer.py:13-21,
+ * torch.optim.Adam arithmetic with the learning rate and bias corrections of this step from the
+ * host), then densities < 0 -> 0, optional quaternion and lobe-axis normalisation and the log-scale
+ * clamp to [min_scale (filter_3D), max_scale] (scripts/train.py:166-181).  Tensors are FP32 with
+ * `width` floats per Gaussian (e.g. positions 3, SH 45); an inactive tensor or one without a gradient
+ * is left as it is, like a torch parameter whose .grad is None. */
+#define RG_TAIL_MAX_TENSORS 12
+typedef struct rg_adam_tensor {
+    float* param;
+    const float* grad;
+    float* exp_avg;
+    float* exp_avg_sq;
+    int32_t width;                     /* floats per Gaussian */
+    int32_t active;                    /* 0: skip this tensor at this step */
+    float lr, beta1, beta2, eps;
+    float one_minus_beta1;             /* 1 - beta1 and 1 - beta2, rounded once from the host's */
+    float one_minus_beta2;             /* values (as torch does with its Python scalars) */
+    float bias1;                       /* 1 - beta1^t */
+    float bias2_sqrt;                  /* sqrt(1 - beta2^t) */
+} rg_adam_tensor;
+
+typedef struct rg_train_tail {
+    int64_t n;                         /* Gaussians */
+    int32_t n_tensors;
+    int32_t idx_positions, idx_densities, idx_scales, idx_quaternions, idx_lobe_axis;  /* -1: absent */
+    int32_t normalize_quaternions, normalize_lobe_axis;
+    float max_scale;                   /* upper clamp of the log scales (+inf: none) */
+    const float* min_scale;            /* (N,) lower clamp of the log scales (filter_3D), NULL: none */
+    float* grad_norm_accum;            /* (N,) += |dL/dposition|, NULL: skip */
+    float* num_accum;                  /* (N,) += 1 where the position gradient is non-zero, NULL: skip */
+    float* num_accum_gnv;              /* (N,) same, the not-visible statistic, NULL: skip */
+    /* NULL, or a DEVICE array [n_tensors][4] = {active, lr, bias1, bias2_sqrt} read by the kernel in
+     * place of those host fields (tensors[i].active must still be set for a tensor that may step):
+     * the launch can then be captured in a CUDA graph and each replay's scalars written beforehand. */
+    const float* step_scalars;
+    rg_adam_tensor tensors[RG_TAIL_MAX_TENSORS];
+} rg_train_tail;
+
+RG_API int rg_train_tail_step(const rg_train_tail* d, void* stream);
 
 #ifdef __cplusplus
 }

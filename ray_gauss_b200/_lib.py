@@ -65,6 +65,27 @@ class rg_tuning(ctypes.Structure):
                 ("list_capacity", ctypes.c_int32), ("record_hits", ctypes.c_int32)]
 
 
+RG_TAIL_MAX_TENSORS = 12
+
+
+class rg_adam_tensor(ctypes.Structure):
+    _fields_ = [("param", ctypes.c_void_p), ("grad", ctypes.c_void_p), ("exp_avg", ctypes.c_void_p),
+                ("exp_avg_sq", ctypes.c_void_p), ("width", ctypes.c_int32), ("active", ctypes.c_int32),
+                ("lr", ctypes.c_float), ("beta1", ctypes.c_float), ("beta2", ctypes.c_float), ("eps", ctypes.c_float),
+                ("one_minus_beta1", ctypes.c_float), ("one_minus_beta2", ctypes.c_float),
+                ("bias1", ctypes.c_float), ("bias2_sqrt", ctypes.c_float)]
+
+
+class rg_train_tail(ctypes.Structure):
+    _fields_ = [("n", ctypes.c_int64), ("n_tensors", ctypes.c_int32), ("idx_positions", ctypes.c_int32),
+                ("idx_densities", ctypes.c_int32), ("idx_scales", ctypes.c_int32), ("idx_quaternions", ctypes.c_int32),
+                ("idx_lobe_axis", ctypes.c_int32), ("normalize_quaternions", ctypes.c_int32),
+                ("normalize_lobe_axis", ctypes.c_int32), ("max_scale", ctypes.c_float), ("min_scale", ctypes.c_void_p),
+                ("grad_norm_accum", ctypes.c_void_p), ("num_accum", ctypes.c_void_p),
+                ("num_accum_gnv", ctypes.c_void_p), ("step_scalars", ctypes.c_void_p),
+                ("tensors", rg_adam_tensor * RG_TAIL_MAX_TENSORS)]
+
+
 assert ctypes.sizeof(rg_camera) == 64
 assert ctypes.sizeof(rg_gaussians) == 88
 assert ctypes.sizeof(rg_settings) == 32
@@ -100,6 +121,7 @@ SIGNATURES = {
     "rg_leaf_order": (ctypes.c_int, [_P, _P, _P]),
     "rg_render_forward_noalloc": (ctypes.c_int, [ctypes.POINTER(rg_gaussians), _P, ctypes.c_int32,
                                                  ctypes.POINTER(rg_settings), _P, _P, _P]),
+    "rg_train_tail_step": (ctypes.c_int, [ctypes.POINTER(rg_train_tail), _P]),
 }
 
 _LOCK = threading.Lock()

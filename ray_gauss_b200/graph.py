@@ -13,6 +13,12 @@ Usage::
     for it in range(n):
         step.replay()            # grads in step.grads, loss in step.loss (device tensors)
         optimizer_step(params, step.grads)   # in-place updates of the same tensors
+
+With ``tail=FusedTrainTail(...)`` over the same tensors, the Adam steps, the densification
+statistics and the parameter clamps are captured too (one more kernel), and with
+``activation=point_cloud_data`` the params are the trained tensors of the reference's point cloud:
+``replay()`` is then a whole iteration of the reference loop (scripts/train.py:100-181, L1/SSIM loss
+aside) without host synchronisation.
 """
 from __future__ import annotations
 
@@ -28,12 +34,18 @@ class GraphedStep:
     """Capture fwd+bwd of :class:`BatchedRenderFunction` over fixed parameter/target tensors.
 
     ``params`` are leaf tensors updated in place between replays (their storage must not change);
-    ``target`` is the (R, 3) packed target of the views; ``loss`` is "mse" or "l1".
+    ``target`` is the (R, 3) packed target of the views; ``loss`` is "mse" or "l1".  Without
+    ``activation`` the params are the render inputs (positions, scales, ...); with it they are the
+    trained tensors and ``activation(params)`` gives the render inputs inside the graph (e.g.
+    :func:`ray_gauss_b200.train_tail.point_cloud_data`), and ``grads`` are those of the trained tensors.
+    ``tail`` (a :class:`ray_gauss_b200.train_tail.FusedTrainTail` over tensors of ``params``) and its
+    ``min_scale`` are captured after the backward.
     """
 
     def __init__(self, params: dict, views: BatchedViews, target: torch.Tensor, loss: str = "mse",
-                 warmup: int = 3):
-        self.params = {k: params[k] for k in _KEYS if params.get(k) is not None}
+                 warmup: int = 3, tail=None, min_scale: torch.Tensor | None = None, activation=None):
+        self.activation = activation
+        self.params = self._select(params)
         self.views = views
         self.target = target
         self.loss_kind = loss
@@ -41,11 +53,19 @@ class GraphedStep:
         self.graph = None
         self.loss = None
         self.grads = None
+        self.tail = tail
+        self.min_scale = min_scale
         self._capture()
+
+    def _select(self, params):
+        if self.activation is not None:
+            return {k: v for k, v in params.items() if v is not None}
+        return {k: params[k] for k in _KEYS if params.get(k) is not None}
 
     def _step(self):
         P = self.params
-        out = BatchedRenderFunction.apply(*(P.get(k) for k in _KEYS), self.views)
+        X = P if self.activation is None else self.activation(P)
+        out = BatchedRenderFunction.apply(*(X.get(k) for k in _KEYS), self.views)
         if self.loss_kind == "mse":
             loss = torch.nn.functional.mse_loss(out, self.target)
         else:
@@ -69,16 +89,24 @@ class GraphedStep:
         self.graph = torch.cuda.CUDAGraph()
         with torch.cuda.graph(self.graph):
             loss, grads = self._step()
+            if self.tail is not None:
+                by_id = {id(v): g for v, g in zip(self.params.values(), grads)}
+                missing = [k for k, v in self.tail.params.items() if id(v) not in by_id]
+                if missing:
+                    raise ValueError(f"tail tensors not among the step's parameters: {missing}")
+                self.tail.capture({k: by_id[id(v)] for k, v in self.tail.params.items()}, self.min_scale)
         self.loss = loss
         self.grads = dict(zip(self.params.keys(), grads))
 
     def replay(self):
+        if self.tail is not None:
+            self.tail.prepare_replay()
         self.graph.replay()
         return self.loss
 
     def rebuild(self, params: dict | None = None):
         """Re-capture after the parameter tensors were replaced (e.g. densification)."""
         if params is not None:
-            self.params = {k: params[k] for k in _KEYS if params.get(k) is not None}
+            self.params = self._select(params)
         self.graph = None
         self._capture()

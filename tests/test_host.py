@@ -115,3 +115,78 @@ def test_replica_timing_is_max_over_ranks_gloo():
     out = mgr.dict()
     mp.spawn(_replica, args=(world, _free_port(), out), nprocs=world, join=True)
     assert dict(out) == {0: 15.0, 1: 15.0}
+
+
+def test_train_tail_rejects_bad_arguments_without_a_launch(engine_lib):
+    """rg_train_tail_step validates its descriptor on the host: these return RG_ERR_INVALID_ARG (1)
+    before any device work."""
+    import ctypes
+
+    from ray_gauss_b200 import _lib
+    lib = engine_lib
+    d = _lib.rg_train_tail()
+    d.n_tensors = _lib.RG_TAIL_MAX_TENSORS + 1
+    assert lib.rg_train_tail_step(ctypes.byref(d), None) == 1
+    d = _lib.rg_train_tail()
+    d.n, d.n_tensors = 10, 1
+    d.idx_positions, d.idx_densities, d.idx_scales, d.idx_quaternions, d.idx_lobe_axis = 0, -1, -1, -1, -1
+    d.tensors[0].param, d.tensors[0].width = 0x1000, 4          # positions must be 3 wide
+    assert lib.rg_train_tail_step(ctypes.byref(d), None) == 1
+    d.tensors[0].width, d.tensors[0].active = 3, 1              # active without moments
+    assert lib.rg_train_tail_step(ctypes.byref(d), None) == 1
+    d.tensors[0].exp_avg, d.tensors[0].exp_avg_sq = 0x2000, 0x3000
+    d.tensors[0].bias1, d.tensors[0].bias2_sqrt = 0.0, 1.0      # bias correction of step 0
+    assert lib.rg_train_tail_step(ctypes.byref(d), None) == 1
+    d.idx_positions, d.idx_quaternions, d.normalize_quaternions = -1, 0, 1
+    d.tensors[0].width, d.tensors[0].active, d.tensors[0].param = 4, 0, 0x1004   # unaligned quaternions
+    assert lib.rg_train_tail_step(ctypes.byref(d), None) == 1
+    d.n = 0
+    d.tensors[0].param = 0x1000
+    assert lib.rg_train_tail_step(ctypes.byref(d), None) == 0   # nothing to do
+
+
+@pytest.mark.filterwarnings("ignore:Detected call of")
+def test_lr_schedule_follows_optimizer_manager_logic():
+    """The host-side schedule of the fused tail against torch's Adam + ExponentialLR driven by the
+    reference's manager logic (classes/optimizer.py:13-21), on CPU tensors."""
+    from ray_gauss_b200.train_tail import FusedTrainTail, LrSchedule
+    s = LrSchedule.exponential(1e-2, 1e-4, decay=4, delay=2, donotuse=1)
+    assert abs(s.gamma ** 4 - 1e-2) < 1e-12
+    tail = FusedTrainTail.__new__(FusedTrainTail)
+    tail.names, tail.betas = ["a"], (0.9, 0.999)
+    tail.schedules, tail.lr = {"a": s}, {"a": s.lr}
+    tail.manager_step, tail.adam_step = {"a": 0}, {"a": 0}
+    p = torch.zeros(1, requires_grad=True)
+    opt = torch.optim.Adam([p], lr=s.lr)
+    sch = torch.optim.lr_scheduler.ExponentialLR(opt, gamma=s.gamma)
+    for it in range(9):
+        has = it != 4
+        (_, use, lr, b1c, b2c), = tail._plan(lambda k: has)
+        if it < s.donotuse:
+            assert not use
+            continue
+        assert use == has
+        assert abs(lr - opt.param_groups[0]["lr"]) <= 1e-15
+        if has:
+            t = tail.adam_step["a"]
+            assert abs(b1c - (1 - 0.9 ** t)) < 1e-15 and abs(b2c - (1 - 0.999 ** t) ** 0.5) < 1e-15
+        if s.delay <= it < s.delay + s.decay:
+            sch.step()
+
+
+def test_point_cloud_data_inverts_raw_from_render_inputs():
+    """get_data activations (classes/point_cloud.py:689-739) on CPU tensors: the raw tensors made
+    from render inputs give those inputs back; a zero lobe axis renders as (0, 0, 1)."""
+    from ray_gauss_b200 import synthetic as S
+    from ray_gauss_b200.train_tail import point_cloud_data, raw_from_render_inputs
+    p, _, _ = S.workload("small_object", n=200, seed=2)
+    g = torch.Generator().manual_seed(0)
+    p["sph_gauss_features"] = torch.randn(200, 3, 2, generator=g)
+    p["bandwidth_sharpness"] = torch.rand(200, 2, generator=g) * 3 + 0.2
+    p["lobe_axis"] = torch.nn.functional.normalize(torch.randn(200, 2, 3, generator=g), dim=2)
+    raw = raw_from_render_inputs(p)
+    X = point_cloud_data(raw)
+    for k in X:
+        assert torch.allclose(X[k], p[k], rtol=2e-5, atol=1e-6), k
+    raw["lobe_axis"][5, 1] = 0.0
+    assert torch.equal(point_cloud_data(raw)["lobe_axis"][5, 1], torch.tensor([0.0, 0.0, 1.0]))
