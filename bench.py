@@ -337,6 +337,39 @@ def our_arm(args, rank, world, local):
                           "algorithmic_bytes_per_launch": int(tail_bytes), "achieved_gbs": round(tail_gbs, 1),
                           "peak_gbs": peak, "frac": round(tail_gbs / peak, 4), "bound": "hbm"}}
         views.update = False
+        # densify + prune (every few hundred iterations in the reference) on the trained statistics
+        # of these replays: 80th-percentile gradient threshold, clone/split boundary at the median
+        # scale; one untimed call (the allocator grows to the new size), then three on fresh copies
+        from ray_gauss_b200.densify import densify_and_prune
+        mean_g = tail.stats["xyz_gradient_accum_norm"] / tail.stats["num_accum"].clamp(min=1)
+        thr = float(torch.quantile(mean_g[:1 << 20], 0.8))
+        extent = float(torch.exp(tparams["scales"].detach()).max(dim=1).values[:1 << 20].median()) * 100.0
+        d_ms, d_out = [], None
+        for _ in range(4):
+            dt = FusedTrainTail({k: v.detach().clone() for k, v in tparams.items()},
+                                {k: LrSchedule(1e-5) for k in tparams}, roles=tail.roles)
+            for k in tparams:
+                dt.exp_avg[k].copy_(tail.exp_avg[k])
+                dt.exp_avg_sq[k].copy_(tail.exp_avg_sq[k])
+            for k in tail.stats:
+                dt.stats[k].copy_(tail.stats[k])
+            f3d = torch.full((n, 1), -12.0, device=dev)
+            torch.cuda.synchronize()
+            g0.record()
+            d_out = densify_and_prune(dt, f3d, thr, 0.05, extent)
+            g1.record()
+            torch.cuda.synchronize()
+            d_ms.append(g0.elapsed_time(g1))
+            del dt, f3d
+        floats = sum(v.numel() for v in tparams.values()) // n
+        moved = 2 * d_out["n"] * 4 * (3 * floats + 4)     # each output row: params, moments, stats read + written
+        dens_ms = sorted(d_ms[1:])[1]
+        densify = {"ms": round(dens_ms, 3), "gaussians_in": n, "gaussians_out": d_out["n"],
+                   "cloned": d_out["n_clone"], "split": d_out["n_split"], "pruned": d_out["n_pruned"],
+                   "bytes_moved": int(moved), "achieved_gbs": round(moved / (dens_ms * 1e-3) / 1e9, 1),
+                   "form": "densify_and_prune(): rg_densify_plan (classify + scan + count read-back) + "
+                           "rg_densify_apply (one gather over every tensor, moment and statistic)"}
+        train["densify"] = densify
         del tstep, tleaves, tparams, tail, tgrads
 
     # ---- e2e through the public API: host parameters and targets in, loss out ----

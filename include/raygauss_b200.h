@@ -30,6 +30,8 @@
  *   rg_render_inference the inference render of scripts/test.py:42-132 (bbox, GAS, colour, launch)
  *   rg_train_tail_step  the step tail of scripts/train.py:121-181 (statistics, the optimizer
  *                       managers' Adam steps of classes/optimizer.py:13-21, parameter clamps)
+ *   rg_densify_plan /   densify_and_prune, classes/point_cloud.py:1068-1143, with the optimizer
+ *   rg_densify_apply    state surgery of classes/optimizer.py:54-83
  */
 #ifndef RAYGAUSS_B200_H
 #define RAYGAUSS_B200_H
@@ -287,6 +289,61 @@ typedef struct rg_train_tail {
 } rg_train_tail;
 
 RG_API int rg_train_tail_step(const rg_train_tail* d, void* stream);
+
+/* ---- Densification (classes/point_cloud.py:1068-1143) -------------------------------------------
+ * densify_and_prune(max_grad, min_density, extent): Gaussians whose mean position gradient
+ * (grad_accum / num_accum, NaN -> 0) is >= grad_threshold are cloned when max(exp(log_scales)) <=
+ * scale_threshold (0.01 * extent; the original and the clone get half the density) and split into
+ * n_split copies otherwise (positions mu + R(q) (z * exp(s)) with z the caller's standard normals,
+ * log scales log(exp(s) * split_scale_mul), half the density; the original is removed); then every
+ * Gaussian with density <= min_density is removed.  Output order as the reference's: surviving
+ * originals, clones, split copy 0 of every split Gaussian, copy 1, ...
+ *   rg_densify_plan   classifies and counts; reads the counts back (synchronises `stream`) and
+ *                     fills n_out and the other counts
+ *   rg_densify_apply  writes every listed tensor at the new size (dst holds n_out rows); draws
+ *                     nothing: split_normals is (n_split * n_split_sel, 3), row c * n_split_sel + k
+ *                     for copy c of the k-th split Gaussian (torch.normal's sample order)
+ * workspace: rg_densify_workspace_bytes(n, n_split) device bytes, kept from plan to apply. */
+#define RG_DENSIFY_MAX_TENSORS 48
+enum rg_densify_kind {
+    RG_DENSIFY_COPY = 0,        /* every output row copies its source row (parameters, filter_3D) */
+    RG_DENSIFY_OLD_ONLY = 1,    /* rows of kept originals move, new rows are 0 (Adam moments, num_accum_gnv) */
+    RG_DENSIFY_ZERO = 2,        /* all rows 0 (the reset gradient statistics); src unused */
+    RG_DENSIFY_DENSITIES = 3,   /* width 1: halved for clones, their originals and split copies */
+    RG_DENSIFY_LOG_SCALES = 4,  /* width 3: split copies get log(exp(s) * split_scale_mul) */
+    RG_DENSIFY_POSITIONS = 5    /* width 3: split copies get mu + R(q) (z * exp(s)) */
+};
+typedef struct rg_densify_tensor {
+    const float* src;                  /* (n, width) */
+    float* dst;                        /* (n_out, width) */
+    int32_t width;
+    int32_t kind;                      /* rg_densify_kind */
+} rg_densify_tensor;
+
+typedef struct rg_densify {
+    int64_t n;
+    const float* grad_accum;           /* (n,) xyz_gradient_accum_norm */
+    const float* num_accum;            /* (n,) */
+    const float* log_scales;           /* (n, 3) */
+    const float* quaternions;          /* (n, 4), 16-byte aligned (split rotations) */
+    const float* densities;            /* (n,) */
+    float grad_threshold;              /* densify_grad_threshold */
+    float scale_threshold;             /* 0.01 * scene extent, rounded to float */
+    float min_density;                 /* SIGMA_THRESHOLD: densities <= it are removed */
+    float split_scale_mul;             /* 1 / (0.8 * n_split), rounded to float */
+    int32_t n_split;                   /* copies per split Gaussian (reference: 2), 1..8 */
+    int32_t planned;                   /* set by rg_densify_plan */
+    void* workspace;
+    /* written by rg_densify_plan */
+    int64_t n_clone, n_split_sel;      /* selected for cloning / splitting */
+    int64_t n_out;                     /* Gaussians after densify and prune */
+    int64_t n_kept, kept_clones, kept_splits;  /* surviving originals, clones, copies per split copy */
+} rg_densify;
+
+RG_API int rg_densify_workspace_bytes(int64_t n, int32_t n_split, uint64_t* bytes);
+RG_API int rg_densify_plan(rg_densify* d, void* stream);
+RG_API int rg_densify_apply(const rg_densify* d, const float* split_normals, const rg_densify_tensor* tensors,
+                            int32_t n_tensors, void* stream);
 
 #ifdef __cplusplus
 }

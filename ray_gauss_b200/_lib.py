@@ -86,6 +86,26 @@ class rg_train_tail(ctypes.Structure):
                 ("tensors", rg_adam_tensor * RG_TAIL_MAX_TENSORS)]
 
 
+RG_DENSIFY_MAX_TENSORS = 48
+RG_DENSIFY_COPY, RG_DENSIFY_OLD_ONLY, RG_DENSIFY_ZERO, RG_DENSIFY_DENSITIES, RG_DENSIFY_LOG_SCALES, \
+    RG_DENSIFY_POSITIONS = range(6)
+
+
+class rg_densify_tensor(ctypes.Structure):
+    _fields_ = [("src", ctypes.c_void_p), ("dst", ctypes.c_void_p), ("width", ctypes.c_int32),
+                ("kind", ctypes.c_int32)]
+
+
+class rg_densify(ctypes.Structure):
+    _fields_ = [("n", ctypes.c_int64), ("grad_accum", ctypes.c_void_p), ("num_accum", ctypes.c_void_p),
+                ("log_scales", ctypes.c_void_p), ("quaternions", ctypes.c_void_p), ("densities", ctypes.c_void_p),
+                ("grad_threshold", ctypes.c_float), ("scale_threshold", ctypes.c_float),
+                ("min_density", ctypes.c_float), ("split_scale_mul", ctypes.c_float), ("n_split", ctypes.c_int32),
+                ("planned", ctypes.c_int32), ("workspace", ctypes.c_void_p), ("n_clone", ctypes.c_int64),
+                ("n_split_sel", ctypes.c_int64), ("n_out", ctypes.c_int64), ("n_kept", ctypes.c_int64),
+                ("kept_clones", ctypes.c_int64), ("kept_splits", ctypes.c_int64)]
+
+
 assert ctypes.sizeof(rg_camera) == 64
 assert ctypes.sizeof(rg_gaussians) == 88
 assert ctypes.sizeof(rg_settings) == 32
@@ -122,6 +142,10 @@ SIGNATURES = {
     "rg_render_forward_noalloc": (ctypes.c_int, [ctypes.POINTER(rg_gaussians), _P, ctypes.c_int32,
                                                  ctypes.POINTER(rg_settings), _P, _P, _P]),
     "rg_train_tail_step": (ctypes.c_int, [ctypes.POINTER(rg_train_tail), _P]),
+    "rg_densify_workspace_bytes": (ctypes.c_int, [ctypes.c_int64, ctypes.c_int32, ctypes.POINTER(ctypes.c_uint64)]),
+    "rg_densify_plan": (ctypes.c_int, [ctypes.POINTER(rg_densify), _P]),
+    "rg_densify_apply": (ctypes.c_int, [ctypes.POINTER(rg_densify), _P, ctypes.POINTER(rg_densify_tensor),
+                                        ctypes.c_int32, _P]),
 }
 
 _LOCK = threading.Lock()

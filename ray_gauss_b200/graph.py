@@ -104,9 +104,15 @@ class GraphedStep:
         self.graph.replay()
         return self.loss
 
-    def rebuild(self, params: dict | None = None):
-        """Re-capture after the parameter tensors were replaced (e.g. densification)."""
+    def rebuild(self, params: dict | None = None, tail=None, min_scale: torch.Tensor | None = None):
+        """Re-capture after the parameter tensors were replaced (e.g. densification): the warm-up
+        rebuilds the LBVH for the new number of Gaussians.  ``tail`` / ``min_scale`` replace the
+        captured tail and its lower scale clamp when given."""
         if params is not None:
             self.params = self._select(params)
+        if tail is not None:
+            self.tail = tail
+        if min_scale is not None:
+            self.min_scale = min_scale
         self.graph = None
         self._capture()

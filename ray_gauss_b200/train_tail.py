@@ -135,6 +135,23 @@ class FusedTrainTail:
     def current_lrs(self) -> dict:
         return dict(self.lr)
 
+    def rebind(self, params: dict, exp_avg: dict, exp_avg_sq: dict, stats: dict | None):
+        """Point the tail at new tensors of the same names (after densification changed N): the
+        learning rates, manager and Adam step counters carry over, like the reference's optimizers
+        whose state is pruned and concatenated in place (classes/optimizer.py:54-83).  A captured
+        graph must be re-captured (``GraphedStep.rebuild``)."""
+        if list(params) != self.names:
+            raise ValueError("rebind needs the same tensor names")
+        n = {int(p.shape[0]) for p in params.values()}
+        if len(n) != 1:
+            raise ValueError("all tensors need the same number of Gaussians")
+        self.params, self.exp_avg, self.exp_avg_sq = params, exp_avg, exp_avg_sq
+        self.n = n.pop()
+        if self.stats is not None:
+            self.stats = stats
+        self._graph_grads = None
+        self._grad_copies = []
+
     # ---- per-step host scalars (the optimizer managers' step logic) ----
     def _plan(self, has_grad) -> list:
         """(name, use, lr, bias1, bias2_sqrt) of this step for every tensor; advances the counters:

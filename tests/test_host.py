@@ -190,3 +190,29 @@ def test_point_cloud_data_inverts_raw_from_render_inputs():
         assert torch.allclose(X[k], p[k], rtol=2e-5, atol=1e-6), k
     raw["lobe_axis"][5, 1] = 0.0
     assert torch.equal(point_cloud_data(raw)["lobe_axis"][5, 1], torch.tensor([0.0, 0.0, 1.0]))
+
+
+def test_densify_validates_on_the_host(engine_lib):
+    """The densify entry points reject bad descriptors before any device work (RG_ERR_INVALID_ARG
+    = 1), size their workspace, and plan an empty cloud without touching a device."""
+    import ctypes
+
+    from ray_gauss_b200 import _lib
+    lib = engine_lib
+    nb = ctypes.c_uint64()
+    assert lib.rg_densify_workspace_bytes(1000, 0, ctypes.byref(nb)) == 1
+    assert lib.rg_densify_workspace_bytes(1000, 2, ctypes.byref(nb)) == 0 and nb.value > 1000 * 28
+    d = _lib.rg_densify()
+    d.n, d.n_split = 10, 2
+    assert lib.rg_densify_plan(ctypes.byref(d), None) == 1                 # no inputs, no workspace
+    d.n = 0
+    assert lib.rg_densify_plan(ctypes.byref(d), None) == 0 and d.planned == 1 and d.n_out == 0
+    t = (_lib.rg_densify_tensor * 1)()
+    t[0].width, t[0].kind = 2, _lib.RG_DENSIFY_POSITIONS                   # positions are 3 wide
+    assert lib.rg_densify_apply(ctypes.byref(d), None, t, 1, None) == 1
+    t[0].width, t[0].kind = 1, 9                                           # unknown kind
+    assert lib.rg_densify_apply(ctypes.byref(d), None, t, 1, None) == 1
+    t[0].kind = _lib.RG_DENSIFY_DENSITIES
+    assert lib.rg_densify_apply(ctypes.byref(d), None, t, 1, None) == 0    # nothing to write
+    d.planned = 0
+    assert lib.rg_densify_apply(ctypes.byref(d), None, t, 1, None) == 1    # apply before plan
