@@ -32,6 +32,8 @@
  *                       managers' Adam steps of classes/optimizer.py:13-21, parameter clamps)
  *   rg_densify_plan /   densify_and_prune, classes/point_cloud.py:1068-1143, with the optimizer
  *   rg_densify_apply    state surgery of classes/optimizer.py:54-83
+ *   rg_records_to_columns  the field extraction of scripts/ply.py:85-146 (read_ply) and of the
+ *                       loaders classes/point_cloud.py:298-394, 396-495
  */
 #ifndef RAYGAUSS_B200_H
 #define RAYGAUSS_B200_H
@@ -339,6 +341,30 @@ typedef struct rg_densify {
     int64_t n_out;                     /* Gaussians after densify and prune */
     int64_t n_kept, kept_clones, kept_splits;  /* surviving originals, clones, copies per split copy */
 } rg_densify;
+
+/* ---- PLY vertex records -> FP32 columns (scripts/ply.py:85-146) ------------------------------------
+ * `records` is the device copy of a binary PLY vertex block: n records of record_bytes bytes.  Each
+ * field reads `type` at byte `offset` of every record (big_endian: the file's byte order), converts
+ * it to double, optionally applies ((v / div) + add) * mul_a * mul_b in double (the reference's
+ * colour initialisation, classes/point_cloud.py:326-329), and writes it rounded to float to
+ * dst[i * dst_stride].  record_bytes <= 49152; up to RG_RECORD_MAX_FIELDS fields per call. */
+#define RG_RECORD_MAX_FIELDS 1024
+enum rg_field_type {
+    RG_FIELD_I8 = 0, RG_FIELD_U8 = 1, RG_FIELD_I16 = 2, RG_FIELD_U16 = 3,
+    RG_FIELD_I32 = 4, RG_FIELD_U32 = 5, RG_FIELD_F32 = 6, RG_FIELD_F64 = 7
+};
+typedef struct rg_record_field {
+    int32_t offset;                    /* byte offset in the record */
+    int32_t type;                      /* rg_field_type */
+    int32_t big_endian;
+    int32_t affine;                    /* 0: plain conversion */
+    float* dst;
+    int64_t dst_stride;                /* floats between consecutive records' values */
+    double div, add, mul_a, mul_b;
+} rg_record_field;
+
+RG_API int rg_records_to_columns(const void* records, int64_t n, int32_t record_bytes, const rg_record_field* fields,
+                                 int32_t n_fields, void* stream);
 
 RG_API int rg_densify_workspace_bytes(int64_t n, int32_t n_split, uint64_t* bytes);
 RG_API int rg_densify_plan(rg_densify* d, void* stream);

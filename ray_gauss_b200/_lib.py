@@ -86,6 +86,17 @@ class rg_train_tail(ctypes.Structure):
                 ("tensors", rg_adam_tensor * RG_TAIL_MAX_TENSORS)]
 
 
+RG_RECORD_MAX_FIELDS = 1024
+RG_FIELD_I8, RG_FIELD_U8, RG_FIELD_I16, RG_FIELD_U16, RG_FIELD_I32, RG_FIELD_U32, RG_FIELD_F32, RG_FIELD_F64 = range(8)
+
+
+class rg_record_field(ctypes.Structure):
+    _fields_ = [("offset", ctypes.c_int32), ("type", ctypes.c_int32), ("big_endian", ctypes.c_int32),
+                ("affine", ctypes.c_int32), ("dst", ctypes.c_void_p), ("dst_stride", ctypes.c_int64),
+                ("div", ctypes.c_double), ("add", ctypes.c_double), ("mul_a", ctypes.c_double),
+                ("mul_b", ctypes.c_double)]
+
+
 RG_DENSIFY_MAX_TENSORS = 48
 RG_DENSIFY_COPY, RG_DENSIFY_OLD_ONLY, RG_DENSIFY_ZERO, RG_DENSIFY_DENSITIES, RG_DENSIFY_LOG_SCALES, \
     RG_DENSIFY_POSITIONS = range(6)
@@ -142,6 +153,8 @@ SIGNATURES = {
     "rg_render_forward_noalloc": (ctypes.c_int, [ctypes.POINTER(rg_gaussians), _P, ctypes.c_int32,
                                                  ctypes.POINTER(rg_settings), _P, _P, _P]),
     "rg_train_tail_step": (ctypes.c_int, [ctypes.POINTER(rg_train_tail), _P]),
+    "rg_records_to_columns": (ctypes.c_int, [_P, ctypes.c_int64, ctypes.c_int32, ctypes.POINTER(rg_record_field),
+                                             ctypes.c_int32, _P]),
     "rg_densify_workspace_bytes": (ctypes.c_int, [ctypes.c_int64, ctypes.c_int32, ctypes.POINTER(ctypes.c_uint64)]),
     "rg_densify_plan": (ctypes.c_int, [ctypes.POINTER(rg_densify), _P]),
     "rg_densify_apply": (ctypes.c_int, [ctypes.POINTER(rg_densify), _P, ctypes.POINTER(rg_densify_tensor),
