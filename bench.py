@@ -370,6 +370,40 @@ def our_arm(args, rank, world, local):
                    "form": "densify_and_prune(): rg_densify_plan (classify + scan + count read-back) + "
                            "rg_densify_apply (one gather over every tensor, moment and statistic)"}
         train["densify"] = densify
+        # scene I/O: this cloud as a trained-scene PLY (the reference's convertpth_to_ply layout),
+        # loaded back: wall time of load_trained_ply (page-cache read into pinned memory, one copy,
+        # one conversion kernel) and the conversion kernel alone on CUDA events
+        import tempfile
+        from ray_gauss_b200.io import PlyVertices, load_trained_ply, write_trained_ply
+        with tempfile.TemporaryDirectory() as td:
+            nsg_t = tleaves["bandwidth_sharpness"].shape[1]
+            hn = tleaves["spherical_harmonics"].shape[2] + 1
+            path = write_trained_ply(f"{td}/scene.ply", tleaves, hn, nsg_t, tail.stats["xyz_gradient_accum_norm"])
+            fsize = os.path.getsize(path)
+            load_trained_ply(path, dev)
+            torch.cuda.synchronize()
+            w0 = time.perf_counter()
+            loaded = load_trained_ply(path, dev)
+            torch.cuda.synchronize()
+            load_s = time.perf_counter() - w0
+            same = all(torch.equal(loaded["params"][k], tleaves[k].detach()) for k in tleaves)
+            ply = PlyVertices(path, dev)
+            cols = torch.empty((ply.n, len(ply.names)), dtype=torch.float32, device=dev)
+            targets = [(nm, cols[:, j], None) for j, nm in enumerate(ply.names)]
+            ply.fill(targets)
+            torch.cuda.synchronize()
+            g0.record()
+            ply.fill(targets)
+            g1.record()
+            torch.cuda.synchronize()
+            k_ms = g0.elapsed_time(g1)
+            del loaded, ply, cols
+        train["scene_io"] = {"file_bytes": int(fsize), "load_trained_ply_ms": round(load_s * 1e3, 2),
+                             "load_gbs": round(fsize / load_s / 1e9, 2), "round_trip_equal": bool(same),
+                             "records_to_columns_ms": round(k_ms, 3),
+                             "records_to_columns_gbs": round(2 * fsize / (k_ms * 1e-3) / 1e9, 1),
+                             "form": "write_trained_ply then load_trained_ply of the 1M-Gaussian cloud; kernel: "
+                                     "every field of every record read once and written once"}
         del tstep, tleaves, tparams, tail, tgrads
 
     # ---- e2e through the public API: host parameters and targets in, loss out ----

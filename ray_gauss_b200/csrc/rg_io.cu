@@ -17,7 +17,9 @@ namespace {
 
 constexpr int kIoThreads = 256;
 constexpr int kIoSmem = 48 * 1024;
-constexpr int kFieldsPerLaunch = 48;   // 3 KB of field descriptors in the kernel parameters
+// 10 KB of field descriptors in the kernel parameters (CUDA 12.1+ allows 32 KB on sm_70 and later):
+// a trained scene's ~116 fields take one launch, so the records are staged once
+constexpr int kFieldsPerLaunch = 160;
 
 struct IoArgs {
     rg_record_field f[kFieldsPerLaunch];
@@ -65,9 +67,10 @@ __global__ void __launch_bounds__(kIoThreads) k_records_to_columns(const IoArgs 
         for (long long i = threadIdx.x; i < bytes; i += kIoThreads) tile[i] = src[i];
     }
     __syncthreads();
-    // consecutive threads take consecutive records of one field
+    // consecutive threads take consecutive fields of one record: the fields of a tensor row are
+    // consecutive in the file (x y z, sh0r sh1r .., sx sy sz), so the stores coalesce
     for (int i = threadIdx.x; i < nr * a.n_fields; i += kIoThreads) {
-        const int fi = i / nr, r = i - fi * nr;
+        const int r = i / a.n_fields, fi = i - r * a.n_fields;
         const rg_record_field& f = a.f[fi];
         double v = field_value(tile + (long long)r * a.record_bytes + f.offset, f.type, f.big_endian != 0);
         float out;
