@@ -34,6 +34,7 @@
  *   rg_densify_apply    state surgery of classes/optimizer.py:54-83
  *   rg_records_to_columns  the field extraction of scripts/ply.py:85-146 (read_ply) and of the
  *                       loaders classes/point_cloud.py:298-394, 396-495
+ *   rg_compute_3d_filter   PointCloud.compute_3D_filter, classes/point_cloud.py:1153-1215
  */
 #ifndef RAYGAUSS_B200_H
 #define RAYGAUSS_B200_H
@@ -365,6 +366,26 @@ typedef struct rg_record_field {
 
 RG_API int rg_records_to_columns(const void* records, int64_t n, int32_t record_bytes, const rg_record_field* fields,
                                  int32_t n_fields, void* stream);
+
+/* ---- 3D minimum-size filter (classes/point_cloud.py:1153-1215) -----------------------------------
+ * filter_out[i] = log(0.5 * depth_i / focal) with depth_i the smallest camera-space depth over the
+ * cameras that see Gaussian i (depth > 0.2, projection inside the image widened by 15 % per side),
+ * or the largest such depth of all Gaussians when no camera sees it (-inf when no Gaussian is seen
+ * at all; the reference raises).  Each camera holds the reference's per-camera values rounded to
+ * float on the host: R (world_view_transform[:3,:3], row-major), T (world_view_transform[3,:3]),
+ * focal_x, focal_y, W / 2, H / 2 and the window bounds -0.15 W, 1.15 W, -0.15 H, 1.15 H.
+ * inv_focal = 1 / (largest focal length), rounded to float.  depth_scratch: n floats and
+ * max_scratch: one word of device memory. */
+typedef struct rg_filter_camera {
+    float R[9];
+    float T[3];
+    float focal_x, focal_y, cx, cy;
+    float x_lo, x_hi, y_lo, y_hi;
+} rg_filter_camera;
+
+RG_API int rg_compute_3d_filter(const float* positions, int64_t n, const rg_filter_camera* cameras, int32_t n_cams,
+                                float inv_focal, float* depth_scratch, uint32_t* max_scratch, float* filter_out,
+                                void* stream);
 
 RG_API int rg_densify_workspace_bytes(int64_t n, int32_t n_split, uint64_t* bytes);
 RG_API int rg_densify_plan(rg_densify* d, void* stream);

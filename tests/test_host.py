@@ -216,3 +216,26 @@ def test_densify_validates_on_the_host(engine_lib):
     assert lib.rg_densify_apply(ctypes.byref(d), None, t, 1, None) == 0    # nothing to write
     d.planned = 0
     assert lib.rg_densify_apply(ctypes.byref(d), None, t, 1, None) == 1    # apply before plan
+
+
+def test_filter3d_camera_table_and_validation(engine_lib):
+    """The 3D filter's camera rows hold the reference's per-camera values rounded to float
+    (classes/point_cloud.py:1170-1196), and the entry point rejects missing buffers on the host."""
+    import ctypes
+
+    import numpy as np
+
+    from ray_gauss_b200 import synthetic as S
+    from ray_gauss_b200.filter3d import camera_table, fov2focal
+    cams = S.ring_cameras(3, seed=1)
+    table, focal = camera_table(cams)
+    assert table.shape == (3, 20) and table.dtype == np.float32
+    c = cams[1]
+    wvt = c.world_view_transform.numpy()
+    assert np.array_equal(table[1, :9], wvt[:3, :3].reshape(-1)) and np.array_equal(table[1, 9:12], wvt[3, :3])
+    assert table[1, 12] == np.float32(fov2focal(c.FoVx, c.image_width))
+    assert table[1, 17] == np.float32(c.image_width * 1.15) and table[1, 18] == np.float32(-0.15 * c.image_height)
+    assert focal == max(max(fov2focal(k.FoVx, k.image_width), fov2focal(k.FoVy, k.image_height)) for k in cams)
+    lib = engine_lib
+    assert lib.rg_compute_3d_filter(None, 10, None, 0, ctypes.c_float(1.0), None, None, None, None) == 1
+    assert lib.rg_compute_3d_filter(None, 0, None, 0, ctypes.c_float(1.0), None, None, None, None) == 0
