@@ -404,6 +404,28 @@ def our_arm(args, rank, world, local):
                              "records_to_columns_gbs": round(2 * fsize / (k_ms * 1e-3) / 1e9, 1),
                              "form": "write_trained_ply then load_trained_ply of the 1M-Gaussian cloud; kernel: "
                                      "every field of every record read once and written once"}
+        # the training loop's other per-Gaussian passes: the 3D filter over this step's cameras
+        # (every 100 iterations) and the k-NN initial scales (once, for clouds without scales)
+        from ray_gauss_b200.filter3d import compute_3D_filter
+        from ray_gauss_b200.knn import dist_cuda2
+        pos = tleaves["positions"].detach().contiguous()
+        compute_3D_filter(pos, cams)
+        dist_cuda2(pos)
+        torch.cuda.synchronize()
+        g0.record()
+        compute_3D_filter(pos, cams)
+        g1.record()
+        torch.cuda.synchronize()
+        f_ms = g0.elapsed_time(g1)
+        g0.record()
+        dist_cuda2(pos)
+        g1.record()
+        torch.cuda.synchronize()
+        k_ms = g0.elapsed_time(g1)
+        train["filter_3D"] = {"ms": round(f_ms, 3), "gaussians": n, "cameras": len(cams),
+                              "form": "compute_3D_filter(): two kernels, cameras in shared memory"}
+        train["knn_scales"] = {"ms": round(k_ms, 3), "points": n,
+                               "form": "dist_cuda2(): Morton sort + warp-shared box search, exact 3-NN"}
         del tstep, tleaves, tparams, tail, tgrads
 
     # ---- e2e through the public API: host parameters and targets in, loss out ----

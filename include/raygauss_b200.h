@@ -35,6 +35,8 @@
  *   rg_records_to_columns  the field extraction of scripts/ply.py:85-146 (read_ply) and of the
  *                       loaders classes/point_cloud.py:298-394, 396-495
  *   rg_compute_3d_filter   PointCloud.compute_3D_filter, classes/point_cloud.py:1153-1215
+ *   rg_knn_mean_dist    distCUDA2 of the simple-knn extension (submodules/simple-knn/spatial.cu:14-25),
+ *                       used by classes/point_cloud.py:374-378 for point clouds without scales
  */
 #ifndef RAYGAUSS_B200_H
 #define RAYGAUSS_B200_H
@@ -348,7 +350,7 @@ typedef struct rg_densify {
  * field reads `type` at byte `offset` of every record (big_endian: the file's byte order), converts
  * it to double, optionally applies ((v / div) + add) * mul_a * mul_b in double (the reference's
  * colour initialisation, classes/point_cloud.py:326-329), and writes it rounded to float to
- * dst[i * dst_stride].  record_bytes <= 49152; up to RG_RECORD_MAX_FIELDS fields per call. */
+ * dst[i * dst_stride].  record_bytes <= 36864; up to RG_RECORD_MAX_FIELDS fields per call. */
 #define RG_RECORD_MAX_FIELDS 1024
 enum rg_field_type {
     RG_FIELD_I8 = 0, RG_FIELD_U8 = 1, RG_FIELD_I16 = 2, RG_FIELD_U16 = 3,
@@ -386,6 +388,14 @@ typedef struct rg_filter_camera {
 RG_API int rg_compute_3d_filter(const float* positions, int64_t n, const rg_filter_camera* cameras, int32_t n_cams,
                                 float inv_focal, float* depth_scratch, uint32_t* max_scratch, float* filter_out,
                                 void* stream);
+
+/* ---- Mean squared distance to the 3 nearest neighbours (simple-knn distCUDA2) --------------------
+ * mean_dist[i] = (d0 + d1 + d2) / 3 with d0 <= d1 <= d2 the three smallest squared distances from
+ * point i to the other points (exact; missing neighbours count as FLT_MAX, so two neighbours give
+ * about FLT_MAX / 3 and one or none +inf, as the extension).  points: (n, 3)
+ * device floats; workspace: rg_knn_workspace_bytes(n) device bytes. */
+RG_API int rg_knn_workspace_bytes(int64_t n, uint64_t* bytes);
+RG_API int rg_knn_mean_dist(const float* points, int64_t n, float* mean_dist, void* workspace, void* stream);
 
 RG_API int rg_densify_workspace_bytes(int64_t n, int32_t n_split, uint64_t* bytes);
 RG_API int rg_densify_plan(rg_densify* d, void* stream);

@@ -156,6 +156,8 @@ SIGNATURES = {
     "rg_records_to_columns": (ctypes.c_int, [_P, ctypes.c_int64, ctypes.c_int32, ctypes.POINTER(rg_record_field),
                                              ctypes.c_int32, _P]),
     "rg_compute_3d_filter": (ctypes.c_int, [_P, ctypes.c_int64, _P, ctypes.c_int32, ctypes.c_float, _P, _P, _P, _P]),
+    "rg_knn_workspace_bytes": (ctypes.c_int, [ctypes.c_int64, ctypes.POINTER(ctypes.c_uint64)]),
+    "rg_knn_mean_dist": (ctypes.c_int, [_P, ctypes.c_int64, _P, _P, _P]),
     "rg_densify_workspace_bytes": (ctypes.c_int, [ctypes.c_int64, ctypes.c_int32, ctypes.POINTER(ctypes.c_uint64)]),
     "rg_densify_plan": (ctypes.c_int, [ctypes.POINTER(rg_densify), _P]),
     "rg_densify_apply": (ctypes.c_int, [ctypes.POINTER(rg_densify), _P, ctypes.POINTER(rg_densify_tensor),

@@ -16,7 +16,7 @@
 namespace {
 
 constexpr int kIoThreads = 256;
-constexpr int kIoSmem = 48 * 1024;
+constexpr int kIoSmem = 36 * 1024;     // record tile; the field descriptors take 10 KB beside it
 // 10 KB of field descriptors in the kernel parameters (CUDA 12.1+ allows 32 KB on sm_70 and later):
 // a trained scene's ~116 fields take one launch, so the records are staged once
 constexpr int kFieldsPerLaunch = 160;
@@ -54,6 +54,10 @@ __device__ double field_value(const unsigned char* p, int type, bool big) {
 
 __global__ void __launch_bounds__(kIoThreads) k_records_to_columns(const IoArgs a) {
     extern __shared__ unsigned char tile[];
+    // descriptors in shared memory: neighbouring lanes read different fields, which from the
+    // kernel parameters would serialise on the constant cache
+    __shared__ rg_record_field fs[kFieldsPerLaunch];
+    for (int i = threadIdx.x; i < a.n_fields; i += kIoThreads) fs[i] = a.f[i];
     const long long r0 = (long long)blockIdx.x * a.tile;
     const int nr = (int)(r0 + a.tile <= a.n ? a.tile : a.n - r0);
     const long long bytes = (long long)nr * a.record_bytes;
@@ -71,13 +75,17 @@ __global__ void __launch_bounds__(kIoThreads) k_records_to_columns(const IoArgs 
     // consecutive in the file (x y z, sh0r sh1r .., sx sy sz), so the stores coalesce
     for (int i = threadIdx.x; i < nr * a.n_fields; i += kIoThreads) {
         const int r = i / a.n_fields, fi = i - r * a.n_fields;
-        const rg_record_field& f = a.f[fi];
-        double v = field_value(tile + (long long)r * a.record_bytes + f.offset, f.type, f.big_endian != 0);
+        const rg_record_field& f = fs[fi];
+        const unsigned char* src_b = tile + (long long)r * a.record_bytes + f.offset;
         float out;
-        if (f.affine) {
-            v = ((v / f.div) + f.add) * f.mul_a * f.mul_b;
-            out = (float)v;
+        if (f.type == RG_FIELD_F32 && !f.affine && ((uintptr_t)src_b & 3) == 0) {
+            // float32 as stored: one aligned word (byte-swapped for big-endian files)
+            unsigned u = *reinterpret_cast<const unsigned*>(src_b);
+            if (f.big_endian) u = __byte_perm(u, 0, 0x0123);
+            out = __uint_as_float(u);
         } else {
+            double v = field_value(src_b, f.type, f.big_endian != 0);
+            if (f.affine) v = ((v / f.div) + f.add) * f.mul_a * f.mul_b;
             out = (float)v;
         }
         f.dst[(r0 + r) * f.dst_stride] = out;

@@ -6,7 +6,8 @@ the device in one transfer, and ``rg_records_to_columns`` converts the requested
 columns of the trained tensors (one kernel, no per-field host copies).
 
 - :func:`load_from_ply`: ``PointCloud.load_from_ply`` (x, y, z, optional density, red/green/blue
-  mapped to the SH DC term, optional sx/sy/sz and qx/qy/qz/qw).
+  mapped to the SH DC term, optional sx/sy/sz (else the k-NN initial scales of
+  :mod:`ray_gauss_b200.knn`) and qx/qy/qz/qw).
 - :func:`load_from_gaussian_splatting`: ``PointCloud.load_from_gaussian_splatting`` (3DGS files).
 - :func:`load_trained_ply` / :func:`write_trained_ply`: the trained-scene layout written by the
   reference's convertpth_to_ply.py (sh{k}{c}, density, sx.., qx.., sg{k}{c}, bandwidth_sharpness{k},
@@ -146,14 +147,14 @@ class PlyVertices:
         for i, (name, dst, affine) in enumerate(targets):
             if name not in h.offsets:
                 raise KeyError(name)
-            if dst.dtype != torch.float32 or dst.numel() != h.n or dst.device != self.device:
-                raise ValueError(f"{name}: destination must be {h.n} float32 values on {self.device}")
+            if dst.dtype != torch.float32 or dst.dim() != 1 or dst.numel() != h.n or dst.device != self.device:
+                raise ValueError(f"{name}: destination must be a 1-D view of {h.n} float32 values on {self.device}")
             f = arr[i]
             f.offset = h.offsets[name]
             f.type = PLY_TYPES[dict(h.properties)[name]][1]
             f.big_endian = int(h.big_endian)
             f.dst = dst.data_ptr()
-            f.dst_stride = dst.stride(0) if dst.dim() == 1 else 1
+            f.dst_stride = dst.stride(0)
             if affine is not None:
                 f.affine = 1
                 f.div, f.add, f.mul_a, f.mul_b = (float(x) for x in affine)
@@ -183,9 +184,9 @@ def _default_filter_3D(n, dev):
 def load_from_ply(path, sh_nb, sg_nb, default_density, device="cuda") -> dict:
     """``PointCloud.load_from_ply`` (classes/point_cloud.py:298-394).  x, y, z are required;
     density defaults to ``default_density``; red/green/blue are required and become the SH DC term
-    ``(c / 255 - 0.5) * 2 * sqrt(pi)`` with zero higher SH and SG terms; sx/sy/sz are required here
-    (the reference initialises missing scales with the simple-knn extension, which this engine does
-    not include); qx/qy/qz/qw default to (1, 0, 0, 0).  Returns ``{"params", "stats", "filter_3D",
+    ``(c / 255 - 0.5) * 2 * sqrt(pi)`` with zero higher SH and SG terms; missing sx/sy/sz become
+    log sqrt of the mean squared distance to the 3 nearest neighbours (the reference's simple-knn
+    initialisation); qx/qy/qz/qw default to (1, 0, 0, 0).  Returns ``{"params", "stats", "filter_3D",
     "harmonic_number", "num_sph_gauss"}``."""
     ply = PlyVertices(path, device)
     n, dev = ply.n, ply.device
@@ -193,9 +194,6 @@ def load_from_ply(path, sh_nb, sg_nb, default_density, device="cuda") -> dict:
         raise ValueError("No x,y,z coordinates in the pointcloud")
     if not all(c in ply for c in ("red", "green", "blue")):
         raise ValueError("No color field in the pointcloud")
-    if not all(c in ply for c in ("sx", "sy", "sz")):
-        raise ValueError("No scale field in the pointcloud: the k-NN scale initialisation (simple-knn distCUDA2) "
-                         "is not part of this engine")
     p = {"positions": ply.columns(["x", "y", "z"])}
     p["densities"] = (ply.column("density") if "density" in ply else
                       torch.full((n,), np.float32(default_density), dtype=torch.float32, device=dev))
@@ -204,7 +202,12 @@ def load_from_ply(path, sh_nb, sg_nb, default_density, device="cuda") -> dict:
     p["sph_gauss_features"] = torch.zeros((n, 3, sg_nb), dtype=torch.float32, device=dev)
     p["bandwidth_sharpness"] = torch.zeros((n, sg_nb), dtype=torch.float32, device=dev)
     p["lobe_axis"] = torch.zeros((n, sg_nb, 3), dtype=torch.float32, device=dev)
-    p["scales"] = ply.columns(["sx", "sy", "sz"])
+    if all(c in ply for c in ("sx", "sy", "sz")):
+        p["scales"] = ply.columns(["sx", "sy", "sz"])
+    else:
+        # log sqrt of the mean squared distance to the 3 nearest neighbours (simple-knn distCUDA2)
+        from .knn import initial_log_scales
+        p["scales"] = initial_log_scales(p["positions"])
     if all(c in ply for c in ("qx", "qy", "qz", "qw")):
         p["quaternions"] = ply.columns(["qx", "qy", "qz", "qw"])
     else:

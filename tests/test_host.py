@@ -239,3 +239,13 @@ def test_filter3d_camera_table_and_validation(engine_lib):
     lib = engine_lib
     assert lib.rg_compute_3d_filter(None, 10, None, 0, ctypes.c_float(1.0), None, None, None, None) == 1
     assert lib.rg_compute_3d_filter(None, 0, None, 0, ctypes.c_float(1.0), None, None, None, None) == 0
+
+
+def test_knn_validates_on_the_host(engine_lib):
+    import ctypes
+    lib = engine_lib
+    nb = ctypes.c_uint64()
+    assert lib.rg_knn_workspace_bytes(1000, ctypes.byref(nb)) == 0 and nb.value > 1000 * 16
+    assert lib.rg_knn_workspace_bytes(-1, ctypes.byref(nb)) == 1
+    assert lib.rg_knn_mean_dist(None, 10, None, None, None) == 1
+    assert lib.rg_knn_mean_dist(None, 0, None, None, None) == 0
