@@ -82,6 +82,43 @@ class LrSchedule:
         return LrSchedule(init_lr, (final_lr / init_lr) ** (1.0 / decay), delay, decay, donotuse)
 
 
+# configuration sections of the reference's optimisation config (utils/optim_utils.py:4-82) -> the
+# trained tensors they drive
+CONFIG_SECTIONS = {"position": "positions", "rgb": "rgb", "sh": "spherical_harmonics", "density": "densities",
+                   "scale": "scales", "quaternion": "quaternions", "sph_gauss_features": "sph_gauss_features",
+                   "bandwidth_sharpness": "bandwidth_sharpness", "lobe_axis": "lobe_axis"}
+
+
+def _cfg(c, key, default=None):
+    if isinstance(c, dict):
+        return c.get(key, default)
+    return getattr(c, key, default)
+
+
+def schedules_from_config(config_opti) -> dict:
+    """The learning-rate schedules of ``define_optimizer_manager`` (utils/optim_utils.py:4-82,
+    classes/optimizer.py:203-218) from the reference's ``training.optimization`` config (a dict,
+    OmegaConf node or namespace with one section per tensor): ``scheduler: true`` gives an
+    exponential schedule with the section's ``gamma`` or ``(final_lr / init_lr)^(1 / decay_step)``
+    over ``[delay_step, delay_step + decay_step)``; otherwise a constant ``init_lr``.  Every section's
+    ``donotuse_steps`` carries over.  Keys are the trained tensors' names."""
+    out = {}
+    for section, name in CONFIG_SECTIONS.items():
+        c = _cfg(config_opti, section)
+        if c is None:
+            continue
+        donotuse = int(_cfg(c, "donotuse_steps", 0) or 0)
+        init = float(_cfg(c, "init_lr"))
+        if _cfg(c, "scheduler", False):
+            decay, delay = int(_cfg(c, "decay_step")), int(_cfg(c, "delay_step"))
+            gamma = _cfg(c, "gamma")
+            gamma = float(gamma) if gamma is not None else (float(_cfg(c, "final_lr")) / init) ** (1 / decay)
+            out[name] = LrSchedule(init, gamma, delay, decay, donotuse)
+        else:
+            out[name] = LrSchedule(init, donotuse=donotuse)
+    return out
+
+
 class FusedTrainTail:
     """Adam + statistics + clamps over the Gaussians' raw parameter tensors.
 

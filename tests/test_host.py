@@ -249,3 +249,27 @@ def test_knn_validates_on_the_host(engine_lib):
     assert lib.rg_knn_workspace_bytes(-1, ctypes.byref(nb)) == 1
     assert lib.rg_knn_mean_dist(None, 10, None, None, None) == 1
     assert lib.rg_knn_mean_dist(None, 0, None, None, None) == 0
+
+
+def test_schedules_from_the_reference_config():
+    """configs/base.yml's optimisation section (values restated here) through the manager logic of
+    utils/optim_utils.py:4-82: exponential schedules where `scheduler` is set, constant otherwise."""
+    from types import SimpleNamespace as NS
+
+    from ray_gauss_b200.train_tail import schedules_from_config
+    def sec(sched, init, final, decay, delay=0, donotuse=0, **kw):
+        return NS(scheduler=sched, init_lr=init, final_lr=final, decay_step=decay, delay_step=delay,
+                  donotuse_steps=donotuse, **kw)
+    cfg = NS(density=sec(True, 0.5, 0.0001, 30000), rgb=sec(False, 0.001, 0.001, 0),
+             sh=sec(False, 0.00026, 0.00026, 0, donotuse=5), position=sec(True, 0.000017, 0.000001, 30000, 100),
+             scale=sec(False, 0.0115, 0.0115, 0), quaternion=sec(False, 0.00022, 0.00022, 0),
+             sph_gauss_features=sec(False, 0.00036, 0.00036, 0), bandwidth_sharpness=sec(True, 0.045, 0.0, 10, gamma=0.5),
+             lobe_axis=sec(False, 0.003, 0.003, 0))
+    s = schedules_from_config(cfg)
+    assert set(s) == {"positions", "rgb", "spherical_harmonics", "densities", "scales", "quaternions",
+                      "sph_gauss_features", "bandwidth_sharpness", "lobe_axis"}
+    assert s["densities"].gamma == (0.0001 / 0.5) ** (1 / 30000) and s["densities"].decay == 30000
+    assert s["positions"].delay == 100 and s["positions"].lr == 0.000017
+    assert s["spherical_harmonics"].gamma == 1.0 and s["spherical_harmonics"].donotuse == 5
+    assert s["bandwidth_sharpness"].gamma == 0.5
+    assert schedules_from_config({"rgb": {"scheduler": False, "init_lr": 0.1}})["rgb"].lr == 0.1
