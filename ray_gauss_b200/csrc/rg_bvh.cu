@@ -63,8 +63,9 @@ __global__ void __launch_bounds__(256) k_prepass(long long n, const float* __res
         // m_j = (column j of R) . (x - mu) / s_j
         r.a = make_float4(px, py, pz, d);
         r.r0 = make_float4(MUL(R00, ix), MUL(R10, ix), MUL(R20, ix), 1.f / sqrtf(lg));
-        r.r1 = make_float4(MUL(R01, iy), MUL(R11, iy), MUL(R21, iy), 0.f);
-        r.r2 = make_float4(MUL(R02, iz), MUL(R12, iz), MUL(R22, iz), 0.f);
+        // .w: log2(density) and 1 / density for the fast sample arithmetic (per Gaussian, not per sample)
+        r.r1 = make_float4(MUL(R01, iy), MUL(R11, iy), MUL(R21, iy), lg2_approx(d));
+        r.r2 = make_float4(MUL(R02, iz), MUL(R12, iz), MUL(R22, iz), __fdividef(1.f, d));
         float b[6] = {SUB(px, e0), SUB(py, e1), SUB(pz, e2), ADD(px, e0), ADD(py, e1), ADD(pz, e2)};
         // reference intersection-program conic: s' = s sqrt(log(ratio^2)) (NaN below the threshold)
         float dl_is = __fsqrt_rn(lg);

@@ -119,9 +119,10 @@ __device__ __forceinline__ float lcg_rnd(unsigned& prev) {
     return (float)(prev & 0x00FFFFFFu) / (float)0x01000000;
 }
 
-// Leaf record (leaf order), 64 bytes: {mu.xyz, density}, {M row 0, k}, {M row 1, 0}, {M row 2, 0}
-// where m = M (x - mu) = S^-1 R^T (x - mu) and k = 1/sqrt(log((density/0.1)^2)) scales M to the
-// threshold ellipsoid (forward/gaussians_aabb.cu:341-357).
+// Leaf record (leaf order), 64 bytes: {mu.xyz, density}, {M row 0, k}, {M row 1, log2(density)},
+// {M row 2, 1 / density} where m = M (x - mu) = S^-1 R^T (x - mu) and k = 1/sqrt(log((density/0.1)^2))
+// scales M to the threshold ellipsoid (forward/gaussians_aabb.cu:341-357); the log and reciprocal
+// (SFU approximations) serve the fast sample arithmetic.
 struct __align__(16) LeafRec {
     float4 a, r0, r1, r2;
 };

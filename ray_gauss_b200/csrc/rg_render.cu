@@ -578,7 +578,7 @@ __device__ __forceinline__ int slab_buffers(const WarpSmem<FAST, CAP>& sm, int k
                 float3 vb = r.d * kDt;
                 float3 m0 = f3(dot3(r0, v0), dot3(r1, v0), dot3(r2, v0));
                 float3 mb = f3(dot3(r0, vb), dot3(r1, vb), dot3(r2, vb));
-                float A = fmaf(kNegHalfLog2e, dot3(m0, m0), lg2_approx(dn));
+                float A = fmaf(kNegHalfLog2e, dot3(m0, m0), rec.r1.w);   // r1.w = log2(dens)
                 float B2 = (2.f * kNegHalfLog2e) * dot3(m0, mb), Cq = kNegHalfLog2e * dot3(mb, mb);
                 float3 col = f3(col4.x, col4.y, col4.z);
                 const float gcol = GDOT ? dot3(r.g, col) : 0.f;
@@ -779,7 +779,7 @@ __device__ __forceinline__ void slab_adjoint(const WarpSmem<FAST, CAP>& sm, int 
                 // sum dw F, sum dw h and the moments of u = dw h, then divides by dens once
                 const float3 m0 = f3(dot3(r0, v0), dot3(r1, v0), dot3(r2, v0));
                 const float3 mb = f3(dot3(r0, vb), dot3(r1, vb), dot3(r2, vb));
-                float A = fmaf(kNegHalfLog2e, dot3(m0, m0), lg2_approx(dn));
+                float A = fmaf(kNegHalfLog2e, dot3(m0, m0), rec.r1.w);   // r1.w = log2(dens)
                 float B2 = (2.f * kNegHalfLog2e) * dot3(m0, mb), Cq = kNegHalfLog2e * dot3(mb, mb);
 #pragma unroll
                 for (int i = 0; i < kBuf; ++i) {
@@ -794,7 +794,7 @@ __device__ __forceinline__ void slab_adjoint(const WarpSmem<FAST, CAP>& sm, int 
                         U2 = fmaf(fi * fi, u, U2);
                     }
                 }
-                dd = (U0 != 0.f) ? U0 * __fdividef(1.f, dn) : 0.f;
+                dd = (U0 != 0.f) ? U0 * rec.r2.w : 0.f;                   // r2.w = 1 / dens
             } else {
 #pragma unroll
                 for (int i = 0; i < kBuf; ++i) {
