@@ -1,0 +1,70 @@
+"""Differentiation at scale: the 3M-Gaussian unbounded scene with 4 views at 1920x1080, FP32
+storage, full backward to every parameter.  The backward that replays the forward's checkpointed
+per-chunk hit lists must give the gradients of the backward that traverses the BVH again
+(recomputation), with an identical image.  Gradients are sums of float atomics whose order varies
+from run to run; at this size that alone moves them by about 1e-5 relative L2, so the comparison
+allows four times the difference between two replaying runs (at least 1e-5).  The record's memory
+and both backward times are recorded as test properties.
+
+FP64 finite differences run on the small scenes of test_gpu_features.py: at this size the FP64
+oracle cannot render on the host, and FP32 differences include the jumps of samples crossing the
+density threshold, which the adjoint (like the reference's) does not differentiate."""
+import pytest
+import torch
+
+from helpers import rel_l2
+
+pytestmark = pytest.mark.gpu
+
+KEYS = ("positions", "scales", "quaternions", "densities", "color_features", "sph_gauss_features",
+        "bandwidth_sharpness", "lobe_axis")
+
+
+def test_checkpointed_hit_lists_match_recomputation_at_scale(cuda, record_property):
+    from ray_gauss_b200 import synthetic as S
+    from ray_gauss_b200.batched import BatchedRenderFunction, BatchedViews
+    from ray_gauss_b200.engine import Engine
+    p, cams, white = S.workload("unbounded_3m", seed=0, device="cpu")
+    P = {k: v.to(cuda).contiguous() for k, v in p.items()}
+    cams = [c.to(cuda) for c in cams]
+    assert P["positions"].shape[0] == 3_000_000 and len(cams) == 4
+    assert all((c.image_width, c.image_height) == (1920, 1080) for c in cams)
+    eng = Engine(cuda.index or 0)
+    views = BatchedViews(cams, engine=eng, mode="fast", white_background=white)
+    R = views.n_rays
+    eng.reserve(P["positions"].shape[0], len(cams), R)
+    dL = torch.randn((R, 3), device=cuda, generator=torch.Generator(device=cuda).manual_seed(5)) * 1e-3
+
+    def run(record):
+        eng.set_tuning(record_hits=1 if record else -1)
+        Q = {k: v.detach().clone().requires_grad_(True) for k, v in P.items()}
+        e = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+        torch.cuda.synchronize()
+        eng.status(reset=True)
+        e[0].record()
+        out = BatchedRenderFunction.apply(*(Q[k] for k in KEYS), views)
+        e[1].record()
+        out.backward(dL)
+        e[2].record()
+        torch.cuda.synchronize()
+        st = eng.status(reset=True)
+        return out.detach(), {k: Q[k].grad for k in KEYS}, e[0].elapsed_time(e[1]), e[1].elapsed_time(e[2]), st
+
+    run(True)                                               # warm-up: sizes the record and the scratch
+    out1, g1, f1, b1, st1 = run(True)
+    _, g2, _, _, _ = run(True)                              # the atomics' run-to-run spread
+    out0, g0, f0, b0, st0 = run(False)
+    assert st1["record_overflows"] == 0 and st1["replayed_chunks"] > 0 and st0["replayed_chunks"] == 0
+    assert torch.equal(out0, out1) and torch.isfinite(out0).all()
+    for k in KEYS:
+        assert torch.isfinite(g1[k]).all(), k
+        noise = rel_l2(g2[k].cpu().numpy(), g1[k].cpu().numpy())
+        assert rel_l2(g1[k].cpu().numpy(), g0[k].cpu().numpy()) <= max(1e-5, 4 * noise), (k, noise)
+    assert float(g0["densities"].abs().sum()) > 0
+    record_property("rays", R)
+    record_property("record_mb", round(4 * st1["record_words"] / 2 ** 20, 1))
+    record_property("forward_ms", round(f1, 1))
+    record_property("backward_replay_ms", round(b1, 1))
+    record_property("backward_recompute_ms", round(b0, 1))
+    print(f"3M x 4x1080p: forward {f1:.1f} ms, backward replaying {b1:.1f} ms, recomputing {b0:.1f} ms, "
+          f"record {4 * st1['record_words'] / 2 ** 20:.1f} MB")
