@@ -234,6 +234,16 @@ def our_arm(args, rank, world, local):
     launches = eng.kernel_launches() - launches0
     timers, eng.timers = eng.timers, None
     st = eng.status()
+    # the fine-grained traversal counters come from one more, untimed step of the counting kernels
+    eng.set_tuning(diagnostics=1)
+    eng.status(reset=True)
+    zero(leaves)
+    step_batched(leaves)
+    torch.cuda.synchronize()
+    diag = eng.status(reset=True)
+    eng.set_tuning(diagnostics=0)
+    for k in ("node_visits", "leaf_tests", "list_entries", "slab_steps", "entry_slabs"):
+        st[k] = diag[k] * args.steps          # counters_per_step divides by the step count
     ms_max = max_over_ranks(ms, dev)
     value = world * R / (ms_max * 1e-3) / 1e6
 

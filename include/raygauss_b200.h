@@ -47,7 +47,7 @@
 extern "C" {
 #endif
 
-#define RG_ABI_VERSION 2
+#define RG_ABI_VERSION 3
 
 #if defined(__GNUC__)
 #define RG_API __attribute__((visibility("default")))
@@ -162,6 +162,10 @@ typedef struct rg_tuning {
                                           many entries; parity lists always hold 128 */
     int32_t record_hits;               /* 1: the forward records its hit lists and the backward
                                           replays them (default); -1: the backward traverses */
+    int32_t diagnostics;               /* 1: the render kernels also count node visits, leaf tests,
+                                          list entries, slab steps and entry-slabs (rg_status);
+                                          0 (default): those stay 0 and the kernels hold fewer
+                                          registers */
 } rg_tuning;
 
 typedef struct rg_engine rg_engine;

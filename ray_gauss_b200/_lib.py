@@ -62,7 +62,7 @@ class rg_status(ctypes.Structure):
 
 class rg_tuning(ctypes.Structure):
     _fields_ = [("chunk_slabs", ctypes.c_int32), ("blocks_per_sm", ctypes.c_int32),
-                ("list_capacity", ctypes.c_int32), ("record_hits", ctypes.c_int32)]
+                ("list_capacity", ctypes.c_int32), ("record_hits", ctypes.c_int32), ("diagnostics", ctypes.c_int32)]
 
 
 RG_TAIL_MAX_TENSORS = 12
@@ -182,7 +182,7 @@ def load(path: str = LIB_PATH):
             fn = getattr(lib, name)
             fn.restype = res
             fn.argtypes = args
-        if lib.rg_abi_version() != 2:
+        if lib.rg_abi_version() != 3:
             raise RuntimeError("raygauss_b200 ABI version mismatch")
         _LIB = lib
         return lib

@@ -39,7 +39,7 @@ struct rg_engine {
     const rg_camera* rec_cams = nullptr;
     int rec_n_cams = 0;
     rg_settings rec_settings{};
-    rg_tuning tuning{64, 0, 64, 1};
+    rg_tuning tuning{64, 0, 64, 1, 0};
     unsigned long long launches = 0;
     char last_err[256] = {0};
 };
@@ -199,6 +199,7 @@ int fill_args(rg_engine* e, const rg_camera* cams, const rg_settings* s, rg::Ren
     a.max_prim_slice = s->max_prim_slice > 0 ? s->max_prim_slice : 1024;
     a.iteration = s->iteration;
     a.chunk_slabs = e->tuning.chunk_slabs;
+    a.diag = e->tuning.diagnostics;
     a.work_counter = e->work_counter;
     a.st = e->st;
     return RG_OK;
@@ -281,10 +282,12 @@ int rg_set_tuning(rg_engine* e, const rg_tuning* t) {
         return RG_ERR_INVALID_ARG;
     if (t->blocks_per_sm < 0) return RG_ERR_INVALID_ARG;
     if (t->record_hits < -1 || t->record_hits > 1) return RG_ERR_INVALID_ARG;
+    if (t->diagnostics < 0 || t->diagnostics > 1) return RG_ERR_INVALID_ARG;
     if (t->chunk_slabs) e->tuning.chunk_slabs = t->chunk_slabs;
     if (t->list_capacity) e->tuning.list_capacity = t->list_capacity;
     if (t->record_hits) e->tuning.record_hits = t->record_hits;
     e->tuning.blocks_per_sm = t->blocks_per_sm;
+    e->tuning.diagnostics = t->diagnostics;
     e->rec_valid = false;
     return RG_OK;
 }

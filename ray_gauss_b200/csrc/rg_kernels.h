@@ -62,6 +62,7 @@ struct RenderArgs {
     // conic-space sample stepping (parity arithmetic), optional Gaussians per ray
     int infer;
     int* counts;
+    int diag;                  // 1: count the fine-grained traversal/list statistics (rg_tuning.diagnostics)
 };
 
 cudaError_t launch_prepass(const rg_gaussians* g, GaussRec* rec, float* aabb, int* scene_ord, DevStatus* st,

@@ -316,7 +316,7 @@ __device__ __forceinline__ void clear_occ(WarpSmem<FAST, CAP>& sm, int lane) {
 }
 
 // Adds the tile's counters to the warp's totals and resets them.
-template <bool FAST, int CAP>
+template <bool FAST, int CAP, bool DIAG>
 __device__ __forceinline__ void flush_stats(WarpSmem<FAST, CAP>& sm, WarpStats& ws, unsigned hits, unsigned slabs,
                                             int lane) {
 #pragma unroll
@@ -326,11 +326,13 @@ __device__ __forceinline__ void flush_stats(WarpSmem<FAST, CAP>& sm, WarpStats& 
     }
     if (lane == 0) {
         sm.cnt[0] += ws.traversals;
-        sm.cnt[1] += ws.node_visits;
-        sm.cnt[2] += ws.leaf_tests;
-        sm.cnt[3] += ws.entries;
-        sm.cnt[4] += ws.slab_steps;
-        sm.cnt[5] += ws.entry_slabs;
+        if (DIAG) {
+            sm.cnt[1] += ws.node_visits;
+            sm.cnt[2] += ws.leaf_tests;
+            sm.cnt[3] += ws.entries;
+            sm.cnt[4] += ws.slab_steps;
+            sm.cnt[5] += ws.entry_slabs;
+        }
         sm.cnt[6] += ws.replays;
         sm.cnt[7] += hits;
         sm.cnt[8] += slabs;
@@ -341,11 +343,11 @@ __device__ __forceinline__ void flush_stats(WarpSmem<FAST, CAP>& sm, WarpStats& 
 // Exact leaf test of every active lane for the chunk [tb, seg_hi]: appends the leaf to the warp
 // list when any lane's interval meets one of the chunk's slabs.  Returns false (leaf not taken)
 // when the list is already full.
-template <bool FAST, int CAP>
+template <bool FAST, int CAP, bool DIAG>
 __device__ __forceinline__ bool leaf_entry(WarpSmem<FAST, CAP>& sm, const RenderArgs& a, const RayState& r, bool on,
                                            float seg_hi, int K, int nv, int leaf, int& count, int lane,
                                            WarpStats& ws, bool infer) {
-    ++ws.leaf_tests;
+    if (DIAG) ++ws.leaf_tests;
     int lo = 255, hi = -1;
     if (on) {
         float root1, root2;
@@ -381,10 +383,10 @@ __device__ __forceinline__ bool leaf_entry(WarpSmem<FAST, CAP>& sm, const Render
 }
 
 // Publishes the chunk list: occupancy bits and the entry masks per block of MB slabs.
-template <bool FAST, int CAP>
+template <bool FAST, int CAP, bool DIAG>
 __device__ __forceinline__ void finish_list(WarpSmem<FAST, CAP>& sm, int count, int K, int lane, WarpStats& ws) {
     __syncwarp();
-    ws.entries += count;
+    if (DIAG) ws.entries += count;
     // lane l fills blocks l, l+32
     constexpr int MB = WarpSmem<FAST, CAP>::MB;
     const int nblk = (K + MB - 1) / MB;
@@ -409,7 +411,7 @@ __device__ __forceinline__ void finish_list(WarpSmem<FAST, CAP>& sm, int count, 
 // Warp-cooperative traversal for the chunk [tb, seg_hi] of every active lane.  Appends hit leaves
 // with index > cursor to the warp list; returns the entry count.  `ovf` is set when the list
 // filled up before the traversal finished.
-template <bool FAST, int CAP>
+template <bool FAST, int CAP, bool DIAG>
 __device__ int traverse(WarpSmem<FAST, CAP>& sm, const RenderArgs& a, const RayState& r, bool on, float seg_hi,
                         int K, int nv, int cursor, bool& ovf, int lane, WarpStats& ws, bool infer) {
     int count = 0;
@@ -427,7 +429,7 @@ __device__ int traverse(WarpSmem<FAST, CAP>& sm, const RenderArgs& a, const RayS
         }
         if (cur >= 0) {
             // 4-wide node: two halves in the binary node format, children in leaf order
-            ++visits;
+            if (DIAG) ++visits;
             const Node* np = a.nodes4 + 2 * (long long)cur;
             float ab0[6], ab1[6], bb0[6], bb1[6];
             int4 na, nb;
@@ -457,7 +459,7 @@ __device__ int traverse(WarpSmem<FAST, CAP>& sm, const RenderArgs& a, const RayS
             }
         } else {
             int leaf = ~cur;
-            if (leaf > cursor && !leaf_entry<FAST, CAP>(sm, a, r, on, seg_hi, K, nv, leaf, count, lane, ws, infer)) {
+            if (leaf > cursor && !leaf_entry<FAST, CAP, DIAG>(sm, a, r, on, seg_hi, K, nv, leaf, count, lane, ws, infer)) {
                 ovf = true;
                 break;
             }
@@ -465,14 +467,14 @@ __device__ int traverse(WarpSmem<FAST, CAP>& sm, const RenderArgs& a, const RayS
         if (sp == 0) break;
         cur = sm.stack[--sp];
     }
-    ws.node_visits += visits;
-    finish_list<FAST, CAP>(sm, count, K, lane, ws);
+    if (DIAG) ws.node_visits += visits;
+    finish_list<FAST, CAP, DIAG>(sm, count, K, lane, ws);
     return count;
 }
 
 // The chunk list from the forward's record: the recorded leaves (at most the list capacity) get
 // the same exact leaf test as in a traversal, without the traversal.
-template <bool FAST, int CAP>
+template <bool FAST, int CAP, bool DIAG>
 __device__ int replay_list(WarpSmem<FAST, CAP>& sm, const RenderArgs& a, const RayState& r, bool on, float seg_hi,
                            int K, int nv, const unsigned* ids, int n, int lane, WarpStats& ws) {
     int count = 0;
@@ -485,10 +487,10 @@ __device__ int replay_list(WarpSmem<FAST, CAP>& sm, const RenderArgs& a, const R
         for (int j = 0; j < m; ++j) {
             const int leaf = __shfl_sync(kFull, mine, j);
             if (leaf >= 0 && leaf < a.n_leaves)
-                leaf_entry<FAST, CAP>(sm, a, r, on, seg_hi, K, nv, leaf, count, lane, ws, false);
+                leaf_entry<FAST, CAP, DIAG>(sm, a, r, on, seg_hi, K, nv, leaf, count, lane, ws, false);
         }
     }
-    finish_list<FAST, CAP>(sm, count, K, lane, ws);
+    finish_list<FAST, CAP, DIAG>(sm, count, K, lane, ws);
     return count;
 }
 
@@ -549,7 +551,7 @@ __device__ __forceinline__ bool lane_has_entry(const WarpSmem<FAST, CAP>& sm, co
 
 // Sample buffers of slab k: sum of density and density-weighted colour of the lane's hits.  The
 // backward (GDOT) needs the colour only through g . C, so it accumulates that scalar in gC instead.
-template <bool FAST, int CAP, bool GDOT>
+template <bool FAST, int CAP, bool GDOT, bool DIAG>
 __device__ __forceinline__ int slab_buffers(const WarpSmem<FAST, CAP>& sm, int k, int K, bool has, const RayState& r,
                                             const RenderArgs& a, int rgb_base, const float* roff,
                                             float* sig, float3* C, float* gC, int nw, int lane, WarpStats& ws) {
@@ -561,7 +563,7 @@ __device__ __forceinline__ int slab_buffers(const WarpSmem<FAST, CAP>& sm, int k
             const int e = 32 * w + __ffs(mw) - 1;
             mw &= mw - 1u;
             if (!in_urange(sm.urng[e], k)) continue;
-            ++ws.entry_slabs;
+            if (DIAG) ++ws.entry_slabs;
             if (!has) continue;
             const int leaf = sm.ids[e];
             if (!lane_has_entry<FAST, CAP>(sm, a, e, k, K, leaf, r, lane)) continue;
@@ -733,7 +735,7 @@ __device__ __forceinline__ float transpose_reduce16(float* v, int lane) {
 
 // Adjoint of slab k for all list entries: per-lane gradient of each hit Gaussian, warp reduction,
 // one atomic per value.  Value order: ddens, S1.xyz, M2 (xx yy zz xy xz yz), 0, drgb.xyz.
-template <bool FAST, int CAP>
+template <bool FAST, int CAP, bool DIAG>
 __device__ __forceinline__ void slab_adjoint(const WarpSmem<FAST, CAP>& sm, int k, int K, bool has, const RayState& r,
                                              const RenderArgs& a, int rgb_base, const float* roff,
                                              const float* H, const float* F, int nw, int lane,
@@ -747,7 +749,7 @@ __device__ __forceinline__ void slab_adjoint(const WarpSmem<FAST, CAP>& sm, int 
         mw &= mw - 1u;
         if (!in_urange(sm.urng[e], k)) continue;
         const int leaf = sm.ids[e];
-        ++ws.entry_slabs;
+        if (DIAG) ++ws.entry_slabs;
         bool act = has && lane_has_entry<FAST, CAP>(sm, a, e, k, K, leaf, r, lane);
         unsigned am = __ballot_sync(kFull, act);
         if (am == 0u) continue;
@@ -902,7 +904,9 @@ constexpr int min_blocks() {
                 : (BWD ? RG_PAR_BWD_MIN_BLOCKS : RG_PAR_FWD_MIN_BLOCKS);
 }
 
-template <bool BWD, bool FAST, int CAP>
+// DIAG: also count node visits, leaf tests, list entries, slab steps and entry-slabs (rg_status);
+// without it those counters compile away and the kernel holds fewer live registers.
+template <bool BWD, bool FAST, int CAP, bool DIAG>
 __global__ void __launch_bounds__(kWarpsPerBlock * 32, min_blocks<BWD, FAST>()) k_render(RenderArgs a) {
     __shared__ WarpSmem<FAST, CAP> smem[kWarpsPerBlock];
     const int lane = threadIdx.x & 31;
@@ -1044,11 +1048,11 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, min_blocks<BWD, FAST>()) 
             int count;
             if (BWD && rec_cur != kNoRecord && !(rec_hdr & kRecordMulti)) {
                 const unsigned n_ids = min(rec_hdr & 0xffffu, a.rec_cap - rec_cur - 2u);
-                count = replay_list<FAST, CAP>(sm, a, r, on, seg_hi, K, nv, a.rec_arena + rec_cur + 2, (int)n_ids,
+                count = replay_list<FAST, CAP, DIAG>(sm, a, r, on, seg_hi, K, nv, a.rec_arena + rec_cur + 2, (int)n_ids,
                                                lane, ws);
                 ++ws.replays;
             } else {
-                count = traverse<FAST, CAP>(sm, a, r, on, seg_hi, K, nv, -1, ovf, lane, ws, infer);
+                count = traverse<FAST, CAP, DIAG>(sm, a, r, on, seg_hi, K, nv, -1, ovf, lane, ws, infer);
             }
             const unsigned long long* occ = sm.occ;
             if (ovf && K > 1) {
@@ -1096,7 +1100,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, min_blocks<BWD, FAST>()) 
                         k = k2 - 1;
                         continue;
                     }
-                    ++ws.slab_steps;
+                    if (DIAG) ++ws.slab_steps;
                     float roff[kBuf];
                     unsigned seed_next = slab_offsets(a.rnd_sample, r.seed, roff);
                     float sig[kBuf];
@@ -1108,7 +1112,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, min_blocks<BWD, FAST>()) 
                         if (BWD) gC[i] = 0.f;
                         else Cb[i] = f3(0.f, 0.f, 0.f);
                     }
-                    int nh = slab_buffers<FAST, CAP, BWD>(sm, k, K, has, r, a, rgb_base, roff, sig, Cb, gC,
+                    int nh = slab_buffers<FAST, CAP, BWD, DIAG>(sm, k, K, has, r, a, rgb_base, roff, sig, Cb, gC,
                                                           nwords(count), lane, ws);
                     if (has) {
                         ++slabs_acc;
@@ -1124,7 +1128,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, min_blocks<BWD, FAST>()) 
                         float H[kBuf], F[kBuf], Ta, gRa;
                         slab_adjoint_scalars<FAST>(r, sig, gC, H, F, Ta, gRa);
                         bool act = has && nh > 0 && any_density(sig);
-                        slab_adjoint<FAST, CAP>(sm, k, K, act, r, a, rgb_base, roff, H, F, nwords(count), lane, ws);
+                        slab_adjoint<FAST, CAP, DIAG>(sm, k, K, act, r, a, rgb_base, roff, H, F, nwords(count), lane, ws);
                         if (has && nh > 0) {
                             r.T = Ta;
                             r.gR = gRa;
@@ -1152,15 +1156,15 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, min_blocks<BWD, FAST>()) 
                     if (BWD) gC[i] = 0.f;
                     else Cb[i] = f3(0.f, 0.f, 0.f);
                 }
-                int nh = slab_buffers<FAST, CAP, BWD>(sm, 0, 1, has, r, a, rgb_base, roff, sig, Cb, gC, nwords(count),
+                int nh = slab_buffers<FAST, CAP, BWD, DIAG>(sm, 0, 1, has, r, a, rgb_base, roff, sig, Cb, gC, nwords(count),
                                                       lane, ws);
                 bool more = ovf;
                 while (more) {
                     int cursor = sm.ids[count - 1];
                     __syncwarp();
                     if (lane == 0) atomicAdd(&a.st->list_passes, 1ull);
-                    count = traverse<FAST, CAP>(sm, a, r, on, seg_hi, 1, nv, cursor, more, lane, ws, infer);
-                    nh += slab_buffers<FAST, CAP, BWD>(sm, 0, 1, has, r, a, rgb_base, roff, sig, Cb, gC,
+                    count = traverse<FAST, CAP, DIAG>(sm, a, r, on, seg_hi, 1, nv, cursor, more, lane, ws, infer);
+                    nh += slab_buffers<FAST, CAP, BWD, DIAG>(sm, 0, 1, has, r, a, rgb_base, roff, sig, Cb, gC,
                                                        nwords(count), lane, ws);
                 }
                 if (has) {
@@ -1180,8 +1184,8 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, min_blocks<BWD, FAST>()) 
                     int cursor = -1;
                     bool more2 = true;
                     while (more2) {
-                        count = traverse<FAST, CAP>(sm, a, r, on, seg_hi, 1, nv, cursor, more2, lane, ws, infer);
-                        slab_adjoint<FAST, CAP>(sm, 0, 1, act, r, a, rgb_base, roff, H, F, nwords(count), lane, ws);
+                        count = traverse<FAST, CAP, DIAG>(sm, a, r, on, seg_hi, 1, nv, cursor, more2, lane, ws, infer);
+                        slab_adjoint<FAST, CAP, DIAG>(sm, 0, 1, act, r, a, rgb_base, roff, H, F, nwords(count), lane, ws);
                         if (more2) cursor = sm.ids[count - 1];
                         __syncwarp();
                     }
@@ -1199,7 +1203,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, min_blocks<BWD, FAST>()) 
         }
         if (!BWD && rec_here && lane == 0)
             a.rec_tile[tile] = (sm.rec_first == kRecordFailed) ? kNoRecord : sm.rec_first;
-        flush_stats(sm, ws, hits_acc, slabs_acc, lane);
+        flush_stats<FAST, CAP, DIAG>(sm, ws, hits_acc, slabs_acc, lane);
         if (!BWD && valid) {
             const long long ray_g = vt->ray_prefix[view] + (long long)ray_l;
             a.ray_colors[3 * ray_g] = __fadd_rn(r.C.x, __fmul_rn(r.T, bg));
@@ -1277,10 +1281,16 @@ template <bool BWD, bool FAST>
 static cudaError_t launch_cap(int cap, int grid, const RenderArgs& a, cudaStream_t s) {
     const int threads = kWarpsPerBlock * 32;
     if constexpr (FAST) {
-        if (cap <= 64) k_render<BWD, FAST, 256><<<grid, threads, 0, s>>>(a);
-        else k_render<BWD, FAST, 512><<<grid, threads, 0, s>>>(a);
+        if (cap <= 64) {
+            if (a.diag) k_render<BWD, FAST, 256, true><<<grid, threads, 0, s>>>(a);
+            else k_render<BWD, FAST, 256, false><<<grid, threads, 0, s>>>(a);
+        } else {
+            if (a.diag) k_render<BWD, FAST, 512, true><<<grid, threads, 0, s>>>(a);
+            else k_render<BWD, FAST, 512, false><<<grid, threads, 0, s>>>(a);
+        }
     } else {
-        k_render<BWD, FAST, 128><<<grid, threads, 0, s>>>(a);
+        if (a.diag) k_render<BWD, FAST, 128, true><<<grid, threads, 0, s>>>(a);
+        else k_render<BWD, FAST, 128, false><<<grid, threads, 0, s>>>(a);
     }
     return cudaGetLastError();
 }
@@ -1290,10 +1300,10 @@ static int occ_cap(int cap) {
     int nb = 0;
     const int threads = kWarpsPerBlock * 32;
     if constexpr (FAST) {
-        if (cap <= 64) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_render<BWD, FAST, 256>, threads, 0);
-        else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_render<BWD, FAST, 512>, threads, 0);
+        if (cap <= 64) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_render<BWD, FAST, 256, false>, threads, 0);
+        else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_render<BWD, FAST, 512, false>, threads, 0);
     } else {
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_render<BWD, FAST, 128>, threads, 0);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_render<BWD, FAST, 128, false>, threads, 0);
     }
     return nb;
 }

@@ -158,16 +158,24 @@ class Engine:
     def reserve(self, n, n_views=1, n_rays=0):
         check(self.lib.rg_reserve(self.h, int(n), int(n_views), int(n_rays)), self.h, "rg_reserve")
 
-    def set_tuning(self, chunk_slabs=0, blocks_per_sm=0, list_capacity=0, record_hits=0):
-        """0 keeps a value; record_hits 1 / -1 switches the forward's hit-list record on / off."""
-        t = _lib.rg_tuning(int(chunk_slabs), int(blocks_per_sm), int(list_capacity), int(record_hits))
+    def set_tuning(self, chunk_slabs=None, blocks_per_sm=None, list_capacity=None, record_hits=None,
+                   diagnostics=None):
+        """Change the given values and keep the others.  blocks_per_sm 0: as many as fit;
+        record_hits 1 / -1 switches the forward's hit-list record on / off; diagnostics 1 makes the
+        render kernels count node visits, leaf tests, list entries, slab steps and entry-slabs."""
+        cur = self.get_tuning()
+        new = dict(chunk_slabs=chunk_slabs, blocks_per_sm=blocks_per_sm, list_capacity=list_capacity,
+                   record_hits=record_hits, diagnostics=diagnostics)
+        cur.update({k: int(v) for k, v in new.items() if v is not None})
+        t = _lib.rg_tuning(cur["chunk_slabs"], cur["blocks_per_sm"], cur["list_capacity"], cur["record_hits"],
+                           cur["diagnostics"])
         check(self.lib.rg_set_tuning(self.h, ctypes.byref(t)), self.h, "rg_set_tuning")
 
     def get_tuning(self):
         t = _lib.rg_tuning()
         check(self.lib.rg_get_tuning(self.h, ctypes.byref(t)), self.h, "rg_get_tuning")
         return dict(chunk_slabs=t.chunk_slabs, blocks_per_sm=t.blocks_per_sm, list_capacity=t.list_capacity,
-                    record_hits=t.record_hits)
+                    record_hits=t.record_hits, diagnostics=t.diagnostics)
 
     def status(self, reset=False):
         st = _lib.rg_status()

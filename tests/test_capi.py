@@ -61,7 +61,7 @@ def test_struct_layout_matches_c(tmp_path):
 
 
 def test_error_strings_and_abi(engine_lib):
-    assert engine_lib.rg_abi_version() == 2
+    assert engine_lib.rg_abi_version() == 3
     assert engine_lib.rg_error_string(0) == b"ok"
     assert b"invalid" in engine_lib.rg_error_string(1)
     assert engine_lib.rg_error_string(99) == b"unknown error"
