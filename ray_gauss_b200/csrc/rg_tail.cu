@@ -118,7 +118,7 @@ __global__ void __launch_bounds__(kTailThreads) k_train_tail(const TailArgs args
         if (nn == 0.f) { q = make_float4(1.f, 0.f, 0.f, 0.f); nn = 1.f; }
         *qp = make_float4(q.x / nn, q.y / nn, q.z / nn, q.w / nn);
     }
-    if (d.normalize_lobe_axis && d.idx_lobe_axis >= 0) {
+    if (d.normalize_lobe_axis && d.idx_lobe_axis >= 0 && d.tensors[d.idx_lobe_axis].width > 0) {
         const rg_adam_tensor& t = d.tensors[d.idx_lobe_axis];
         for (int l = 0; l < t.width / 3; ++l) {
             float* ax = t.param + g * t.width + 3 * l;
@@ -147,7 +147,9 @@ int check_tail(const rg_train_tail* d) {
         if (idx[j] < -1 || idx[j] >= d->n_tensors) return RG_ERR_INVALID_ARG;
         if (idx[j] >= 0) {
             const rg_adam_tensor& t = d->tensors[idx[j]];
-            if (!t.param || (width[j] > 0 && t.width != width[j]) || (width[j] < 0 && t.width % 3 != 0))
+            // a lobe-axis tensor may have zero width (no SG lobes unlocked yet)
+            if ((!t.param && t.width != 0) || (width[j] > 0 && t.width != width[j]) ||
+                (width[j] < 0 && t.width % 3 != 0))
                 return RG_ERR_INVALID_ARG;
         }
     }

@@ -82,6 +82,36 @@ class LrSchedule:
         return LrSchedule(init_lr, (final_lr / init_lr) ** (1.0 / decay), delay, decay, donotuse)
 
 
+def unlock_spherical_harmonics(tail: "FusedTrainTail", n_sh: int, name: str = "spherical_harmonics"):
+    """``PointCloud.unlock_spherical_harmonics`` (classes/point_cloud.py:518-528): grow the SH
+    coefficients to ``n_sh`` per channel (the DC term lives in rgb) with zeros."""
+    p = tail.params[name]
+    add = n_sh - p.shape[2] - 1
+    if add <= 0:
+        return p
+    return tail.extend(name, torch.zeros((p.shape[0], 3, add), dtype=p.dtype, device=p.device), dim=2)
+
+
+def unlock_spherical_gaussians(tail: "FusedTrainTail", n_sph_gauss: int, generator: torch.Generator | None = None):
+    """``PointCloud.unlock_spherical_gaussians`` (classes/point_cloud.py:530-545): add
+    ``n_sph_gauss`` lobes with zero amplitudes and bandwidths and random (unnormalised, standard
+    normal) axes.  The tail must hold ``sph_gauss_features``, ``bandwidth_sharpness`` and
+    ``lobe_axis`` (zero-width tensors before the first unlock)."""
+    n = tail.n
+    dev = tail.params["sph_gauss_features"].device
+    tail.extend("sph_gauss_features", torch.zeros((n, 3, n_sph_gauss), device=dev), dim=2)
+    tail.extend("bandwidth_sharpness", torch.zeros((n, n_sph_gauss), device=dev), dim=1)
+    axes = torch.randn((n, n_sph_gauss, 3), device=dev, generator=generator)
+    tail.extend("lobe_axis", axes, dim=1)
+
+
+def reset_density(tail: "FusedTrainTail", max_density: float = 4.0, name: str = "densities"):
+    """``PointCloud.reset_density`` (classes/point_cloud.py:1145-1149): densities clamped to at most
+    ``max_density``, their Adam moments zeroed."""
+    d = tail.params[name].detach()
+    return tail.replace(name, torch.min(d, torch.ones_like(d) * max_density))
+
+
 # configuration sections of the reference's optimisation config (utils/optim_utils.py:4-82) -> the
 # trained tensors they drive
 CONFIG_SECTIONS = {"position": "positions", "rgb": "rgb", "sh": "spherical_harmonics", "density": "densities",
@@ -188,6 +218,36 @@ class FusedTrainTail:
             self.stats = stats
         self._graph_grads = None
         self._grad_copies = []
+
+    def extend(self, name: str, extension: torch.Tensor, dim: int) -> torch.Tensor:
+        """``_cat_tensor`` (classes/optimizer.py:71-83): append ``extension`` to tensor ``name``
+        along ``dim`` (e.g. newly unlocked SH coefficients); the Adam moments grow by zeros, the step
+        count and learning rate stay.  Returns the new tensor (a captured graph must be re-captured)."""
+        p = self.params[name]
+        ext = extension.to(device=p.device, dtype=p.dtype)
+        newp = torch.cat((p.detach(), ext), dim=dim).contiguous().requires_grad_(p.requires_grad)
+        m = torch.cat((self.exp_avg[name], torch.zeros_like(ext)), dim=dim).contiguous()
+        v = torch.cat((self.exp_avg_sq[name], torch.zeros_like(ext)), dim=dim).contiguous()
+        params = dict(self.params)
+        params[name] = newp
+        exp_avg, exp_avg_sq = dict(self.exp_avg), dict(self.exp_avg_sq)
+        exp_avg[name], exp_avg_sq[name] = m, v
+        self.rebind(params, exp_avg, exp_avg_sq, self.stats)
+        return newp
+
+    def replace(self, name: str, values: torch.Tensor) -> torch.Tensor:
+        """``_replace`` (classes/optimizer.py:97-106): new values for tensor ``name`` with zero Adam
+        moments; the step count and learning rate stay."""
+        p = self.params[name]
+        newp = values.detach().to(device=p.device, dtype=p.dtype).contiguous().requires_grad_(p.requires_grad)
+        if newp.shape != p.shape:
+            raise ValueError("replace keeps the shape; use extend or densification to change it")
+        params = dict(self.params)
+        params[name] = newp
+        exp_avg, exp_avg_sq = dict(self.exp_avg), dict(self.exp_avg_sq)
+        exp_avg[name], exp_avg_sq[name] = torch.zeros_like(newp), torch.zeros_like(newp)
+        self.rebind(params, exp_avg, exp_avg_sq, self.stats)
+        return newp
 
     # ---- per-step host scalars (the optimizer managers' step logic) ----
     def _plan(self, has_grad) -> list:

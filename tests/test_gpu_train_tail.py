@@ -196,3 +196,91 @@ def test_graphed_step_with_tail_equals_eager_tail(cuda):
     s_now = trained["scales"].detach()
     assert float(s_now.min()) >= float(min_scale[0]) and float(s_now.max()) <= max_scale
     assert tail_g.adam_step["spherical_harmonics"] == 3 and tail_g.adam_step["positions"] == 5
+
+
+def _cat_state(opt, ext, dim):
+    """The reference's _cat_tensor (classes/optimizer.py:71-83) on a torch Adam."""
+    group = opt.param_groups[0]
+    p = group["params"][0]
+    st = opt.state.get(p, None)
+    with torch.no_grad():
+        newp = torch.cat((p, ext), dim=dim).requires_grad_(True)
+    if st is not None:
+        st["exp_avg"] = torch.cat((st["exp_avg"], torch.zeros_like(ext)), dim=dim)
+        st["exp_avg_sq"] = torch.cat((st["exp_avg_sq"], torch.zeros_like(ext)), dim=dim)
+        del opt.state[p]
+        opt.state[newp] = st
+    group["params"][0] = newp
+    return newp
+
+
+def _replace_state(opt, new):
+    """The reference's _replace (classes/optimizer.py:97-106)."""
+    group = opt.param_groups[0]
+    p = group["params"][0]
+    st = opt.state.get(p, None)
+    st["exp_avg"] = torch.zeros_like(new)
+    st["exp_avg_sq"] = torch.zeros_like(new)
+    del opt.state[p]
+    group["params"][0] = new
+    opt.state[new] = st
+    return new
+
+
+def test_unlocks_and_density_reset_follow_the_reference_state_surgery(cuda):
+    """SH unlocked from zero width, two SG lobes unlocked (axes from the same generator), densities
+    reset (classes/point_cloud.py:518-545, 1145-1149), interleaved with Adam steps: the fused tail
+    against torch Adams whose state the reference's _cat_tensor / _replace rewrite."""
+    from ray_gauss_b200.train_tail import (FusedTrainTail, LrSchedule, reset_density, unlock_spherical_gaussians,
+                                           unlock_spherical_harmonics)
+    n = 3000
+    g = torch.Generator(device="cpu").manual_seed(8)
+    init = {"positions": torch.randn(n, 3, generator=g), "rgb": torch.randn(n, 3, generator=g),
+            "spherical_harmonics": torch.zeros(n, 3, 0), "densities": torch.rand(n, generator=g) * 6,
+            "sph_gauss_features": torch.zeros(n, 3, 0), "bandwidth_sharpness": torch.zeros(n, 0),
+            "lobe_axis": torch.zeros(n, 0, 3)}
+    sched = {k: LrSchedule(1e-3 * (i + 1)) for i, k in enumerate(init)}
+    mine = {k: v.clone().to(cuda).contiguous() for k, v in init.items()}
+    tail = FusedTrainTail(mine, sched, roles={"positions": "positions", "densities": "densities",
+                                              "lobe_axis": "lobe_axis"}, normalize_quaternion=False,
+                          statistics=False)
+    opts = {k: torch.optim.Adam([v.clone().to(cuda).requires_grad_(True)], lr=sched[k].lr, eps=1e-15)
+            for k, v in init.items()}
+    ref = lambda k: opts[k].param_groups[0]["params"][0]  # noqa: E731
+    for it in range(6):
+        if it == 2:
+            unlock_spherical_harmonics(tail, 4)
+            _cat_state(opts["spherical_harmonics"], torch.zeros(n, 3, 3, device=cuda), 2)
+        if it == 3:
+            unlock_spherical_gaussians(tail, 2, generator=torch.Generator(device=cuda).manual_seed(4))
+            _cat_state(opts["sph_gauss_features"], torch.zeros(n, 3, 2, device=cuda), 2)
+            _cat_state(opts["bandwidth_sharpness"], torch.zeros(n, 2, device=cuda), 1)
+            axes = torch.randn((n, 2, 3), device=cuda, generator=torch.Generator(device=cuda).manual_seed(4))
+            _cat_state(opts["lobe_axis"], axes, 1)
+        if it == 4:
+            reset_density(tail)
+            d = ref("densities").detach()
+            _replace_state(opts["densities"], torch.min(d, torch.ones_like(d) * 4.0).contiguous().requires_grad_(True))
+        grads = {}
+        for k in init:
+            shape = tuple(ref(k).shape)
+            grads[k] = torch.randn(shape, generator=g).to(cuda) if ref(k).numel() else None
+        for k in init:
+            ref(k).grad = grads[k]
+            tail.params[k].grad = None if grads[k] is None else grads[k].clone()
+        tail.step()
+        for o in opts.values():
+            o.step()
+        with torch.no_grad():
+            ref("densities")[ref("densities") < 0] = 0
+        torch.cuda.synchronize()
+        for k in init:
+            a, b = tail.params[k].detach(), ref(k).detach()
+            assert a.shape == b.shape, (it, k)
+            assert torch.allclose(a, b, rtol=2e-6, atol=2e-7), (it, k, (a - b).abs().max().item())
+            st = opts[k].state.get(ref(k))
+            if st and st["exp_avg"].numel():
+                assert torch.allclose(tail.exp_avg_sq[k], st["exp_avg_sq"], rtol=2e-6, atol=1e-12), (it, k)
+                assert tail.adam_step[k] == int(st["step"]), (it, k)
+    assert tail.params["spherical_harmonics"].shape == (n, 3, 3) and tail.params["lobe_axis"].shape == (n, 2, 3)
+    assert float(tail.params["densities"].max()) <= 4.0 + 1e-2

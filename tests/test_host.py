@@ -273,3 +273,20 @@ def test_schedules_from_the_reference_config():
     assert s["spherical_harmonics"].gamma == 1.0 and s["spherical_harmonics"].donotuse == 5
     assert s["bandwidth_sharpness"].gamma == 0.5
     assert schedules_from_config({"rgb": {"scheduler": False, "init_lr": 0.1}})["rgb"].lr == 0.1
+
+
+def test_tail_extend_and_replace_keep_counters():
+    """extend / replace rewrite the tensors and moments on the host side and keep the step counts
+    and learning rates (the reference's _cat_tensor / _replace)."""
+    from ray_gauss_b200.train_tail import FusedTrainTail, LrSchedule, reset_density, unlock_spherical_harmonics
+    n = 10
+    P = {"spherical_harmonics": torch.zeros(n, 3, 0), "densities": torch.arange(n, dtype=torch.float32)}
+    tail = FusedTrainTail(P, {k: LrSchedule(0.1) for k in P}, roles={"densities": "densities"})
+    tail.adam_step = {"spherical_harmonics": 3, "densities": 5}
+    tail.exp_avg["densities"].fill_(1.0)
+    sh = unlock_spherical_harmonics(tail, 9)
+    assert sh.shape == (n, 3, 8) and tail.exp_avg["spherical_harmonics"].shape == (n, 3, 8)
+    assert tail.adam_step["spherical_harmonics"] == 3
+    d = reset_density(tail)
+    assert float(d.max()) == 4.0 and float(tail.exp_avg["densities"].abs().sum()) == 0.0
+    assert tail.adam_step["densities"] == 5 and tail.params["densities"] is d
