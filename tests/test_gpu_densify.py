@@ -223,3 +223,25 @@ def test_graphed_step_recaptured_after_densify(cuda):
     assert np.isfinite(float(loss)) and all(int(tail.adam_step[k]) == 6 for k in tail.names)
     assert all(torch.isfinite(x).all() for x in tail.params.values())
     assert float(tail.stats["num_accum"].max()) <= 3.0
+
+
+def test_densify_with_zero_width_sg_tensors_in_the_tail(cuda):
+    """SG tensors held at zero width (no lobe unlocked yet) pass through densification with their
+    new row count, and the tail keeps stepping afterwards."""
+    from ray_gauss_b200.densify import densify_and_prune
+    from ray_gauss_b200.train_tail import FusedTrainTail, LrSchedule
+    raw, m, v, stats, f3d = _cloud(4000, cuda, seed=9, nsg=0)
+    tail = FusedTrainTail({k: raw[k].clone() for k in NAMES}, {k: LrSchedule(1e-3) for k in NAMES}, roles=ROLES)
+    for k in stats:
+        tail.stats[k].copy_(stats[k])
+    out = densify_and_prune(tail, f3d.clone(), 1e-4, 0.1, 1.0)
+    torch.cuda.synchronize()
+    n = out["n"]
+    assert out["n_clone"] > 0 and out["n_split"] > 0
+    assert tail.params["sph_gauss_features"].shape == (n, 3, 0) and tail.params["lobe_axis"].shape == (n, 0, 3)
+    assert tail.exp_avg["bandwidth_sharpness"].shape == (n, 0)
+    for k in NAMES:
+        tail.params[k].grad = torch.ones_like(tail.params[k])
+    tail.step(min_scale=out["filter_3D"])
+    torch.cuda.synchronize()
+    assert all(torch.isfinite(x).all() for x in tail.params.values())
