@@ -25,6 +25,7 @@ from __future__ import annotations
 import torch
 
 from .batched import BatchedRenderFunction, BatchedViews
+from .losses import views_l1_ssim_loss
 
 _KEYS = ("positions", "scales", "quaternions", "densities", "color_features", "sph_gauss_features",
          "bandwidth_sharpness", "lobe_axis")
@@ -34,7 +35,8 @@ class GraphedStep:
     """Capture fwd+bwd of :class:`BatchedRenderFunction` over fixed parameter/target tensors.
 
     ``params`` are leaf tensors updated in place between replays (their storage must not change);
-    ``target`` is the (R, 3) packed target of the views; ``loss`` is "mse" or "l1".  Without
+    ``target`` is the (R, 3) packed target of the views; ``loss`` is "mse", "l1" or "l1_ssim" (the
+    reference's 0.8 L1 + 0.2 (1 - SSIM) per view image, averaged over the views).  Without
     ``activation`` the params are the render inputs (positions, scales, ...); with it they are the
     trained tensors and ``activation(params)`` gives the render inputs inside the graph (e.g.
     :func:`ray_gauss_b200.train_tail.point_cloud_data`), and ``grads`` are those of the trained tensors.
@@ -68,6 +70,8 @@ class GraphedStep:
         out = BatchedRenderFunction.apply(*(X.get(k) for k in _KEYS), self.views)
         if self.loss_kind == "mse":
             loss = torch.nn.functional.mse_loss(out, self.target)
+        elif self.loss_kind == "l1_ssim":
+            loss = views_l1_ssim_loss(out, self.target, self.views)
         else:
             loss = torch.nn.functional.l1_loss(out, self.target)
         grads = torch.autograd.grad(loss, [P[k] for k in P], allow_unused=True)

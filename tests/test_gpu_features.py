@@ -164,3 +164,27 @@ def test_bf16_storage_psnr_against_fp64(cuda, oracle):
     target = ref + noise
     assert abs(psnr(out16, target) - psnr(ref, target)) <= 0.05
     assert abs(psnr(out32, target) - psnr(ref, target)) <= 0.05
+
+
+def test_graphed_step_with_the_reference_loss(cuda):
+    """loss="l1_ssim": the reference's (1 - 0.2) L1 + 0.2 (1 - SSIM) per view image inside the captured
+    graph equals the eager loss, with the same gradients up to the float atomics' order."""
+    from ray_gauss_b200.batched import BatchedRenderFunction
+    from ray_gauss_b200.graph import GraphedStep
+    from ray_gauss_b200.losses import views_l1_ssim_loss
+    P, white = _scene(cuda)
+    views = _views(cuda, mode="fast", white_background=white)
+    target = torch.rand((views.n_rays, 3), device=cuda, generator=torch.Generator(device=cuda).manual_seed(6))
+    leaves = {k: v.clone() for k, v in P.items()}
+    step = GraphedStep(leaves, views, target, loss="l1_ssim")
+    loss = step.replay()
+    torch.cuda.synchronize()
+    Q = {k: v.detach().clone().requires_grad_(True) for k, v in leaves.items()}
+    views.update = True
+    out = BatchedRenderFunction.apply(*(Q[k] for k in KEYS), views)
+    ref = views_l1_ssim_loss(out, target, views)
+    ref.backward()
+    assert abs(loss.item() - ref.item()) <= 1e-6
+    for k in KEYS:
+        if Q[k].grad is not None and Q[k].numel():
+            assert rel_l2(step.grads[k].cpu().numpy(), Q[k].grad.cpu().numpy()) <= 1e-4, k

@@ -1,5 +1,6 @@
 """A training loop in the shape of the reference's scripts/train.py:25-181, run entirely on the
-engine's components: the get_data activations, render, MSE and backward captured with the fused
+engine's components: the get_data activations, render, the reference's L1 + SSIM loss and backward
+captured with the fused
 Adam / statistics / clamp tail in one CUDA graph (schedules from the reference's optimisation config),
 the 3D filter refreshed every 5 iterations, densify and prune, SG lobes unlocked from zero width, the
 density reset, and a checkpoint saved, reloaded and restored into a fresh tail.  Every change of
@@ -46,7 +47,7 @@ def test_training_loop_through_every_component(cuda, tmp_path):
                           normalize_quaternion=True, normalize_lobe_axis=True, max_scale=0.0)
     filt = compute_3D_filter(tail.params["positions"].detach(), cams)
     act = lambda r: point_cloud_data(r, normalized_quaternion=False, normalized_lobe_axis=False)  # noqa: E731
-    step = GraphedStep(dict(tail.params), views, target, tail=tail, min_scale=filt, activation=act)
+    step = GraphedStep(dict(tail.params), views, target, loss="l1_ssim", tail=tail, min_scale=filt, activation=act)
     losses, n0 = [], tail.n
     for it in range(1, 31):
         losses.append(step.replay())

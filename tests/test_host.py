@@ -290,3 +290,22 @@ def test_tail_extend_and_replace_keep_counters():
     d = reset_density(tail)
     assert float(d.max()) == 4.0 and float(tail.exp_avg["densities"].abs().sum()) == 0.0
     assert tail.adam_step["densities"] == 5 and tail.params["densities"] is d
+
+
+def test_l1_ssim_loss_matches_the_reference_functions():
+    """The training loss of scripts/train.py:110-112 (utils/loss_utils.py SSIM) against values and
+    image gradients computed by the reference's own functions (tests/golden/make_loss_golden.py),
+    on the CPU: equal to float rounding."""
+    import numpy as np
+
+    from ray_gauss_b200.losses import l1_loss, l1_ssim_loss, ssim
+    d = np.load(os.path.join(ROOT, "tests", "golden", "loss", "loss_l1_ssim.npz"))
+    for i in range(2):
+        img = torch.from_numpy(d[f"img{i}"]).requires_grad_(True)
+        gt = torch.from_numpy(d[f"gt{i}"])
+        assert abs(l1_loss(img, gt).item() - float(d[f"l1_{i}"])) <= 1e-7
+        assert abs(ssim(img, gt).item() - float(d[f"ssim{i}"])) <= 1e-7
+        loss = l1_ssim_loss(img, gt)
+        assert abs(loss.item() - float(d[f"loss{i}"])) <= 1e-7
+        loss.backward()
+        assert np.allclose(img.grad.numpy(), d[f"grad{i}"], rtol=1e-6, atol=1e-10)
