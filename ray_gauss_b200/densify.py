@@ -39,6 +39,8 @@ def densify_and_prune(tail, filter_3D: torch.Tensor, grad_threshold: float, min_
     pos, ls, quat, dens = (P[roles[r]] for r in ("positions", "scales", "quaternions", "densities"))
     n = tail.n
     dev = pos.device
+    if dev.type != "cuda":
+        raise ValueError("densify_and_prune runs on CUDA tensors")
     lib = _lib.load()
     f3d = filter_3D.reshape(-1)
     if f3d.numel() != n or f3d.dtype != torch.float32 or not f3d.is_contiguous():

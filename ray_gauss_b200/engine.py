@@ -66,6 +66,9 @@ def make_gaussians(positions, scales, quaternions, densities, color_features, sp
     dev = positions.device
     if dev.type != "cuda":
         raise ValueError("the ray caster runs on CUDA tensors only")
+    for t in (scales, quaternions, densities, color_features, sph_gauss_features, bandwidth_sharpness, lobe_axis):
+        if t is not None and t.numel() and t.device != dev:
+            raise ValueError("every Gaussian tensor must be on the positions' CUDA device")
     f32 = lambda t: t.detach().to(torch.float32).contiguous()
     pos, scl, quat = f32(positions), f32(scales), f32(quaternions)
     if quat.data_ptr() % 16:

@@ -48,6 +48,8 @@ def camera_table(cameras):
 def compute_3D_filter(positions: torch.Tensor, cameras) -> torch.Tensor:
     if positions.dtype != torch.float32 or not positions.is_contiguous() or positions.dim() != 2:
         raise ValueError("positions: (N, 3) FP32 contiguous")
+    if not positions.is_cuda:
+        raise ValueError("compute_3D_filter runs on CUDA tensors")
     dev = positions.device
     n = positions.shape[0]
     table, focal = camera_table(cameras)

@@ -116,6 +116,8 @@ class PlyVertices:
     def __init__(self, path, device="cuda"):
         self.header = read_ply_header(path)
         self.device = torch.device(device)
+        if self.device.type != "cuda":
+            raise ValueError("PLY records are converted on a CUDA device")
         h = self.header
         nbytes = h.n * h.record_bytes
         host = torch.empty(nbytes, dtype=torch.uint8, pin_memory=True)

@@ -17,6 +17,8 @@ def dist_cuda2(points: torch.Tensor) -> torch.Tensor:
     one or none +inf)."""
     if points.dtype != torch.float32 or not points.is_contiguous() or points.dim() != 2 or points.shape[1] != 3:
         raise ValueError("points: (N, 3) FP32 contiguous")
+    if not points.is_cuda:
+        raise ValueError("dist_cuda2 runs on CUDA tensors")
     n = points.shape[0]
     lib = _lib.load()
     nb = ctypes.c_uint64()

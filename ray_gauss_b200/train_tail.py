@@ -317,6 +317,8 @@ class FusedTrainTail:
         return m
 
     def _launch(self, d):
+        if not self.params[self.names[0]].is_cuda:
+            raise ValueError("the fused tail runs on CUDA tensors")
         check(self.lib.rg_train_tail_step(ctypes.byref(d), ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)),
               None, "rg_train_tail_step")
 

@@ -309,3 +309,23 @@ def test_l1_ssim_loss_matches_the_reference_functions():
         assert abs(loss.item() - float(d[f"loss{i}"])) <= 1e-7
         loss.backward()
         assert np.allclose(img.grad.numpy(), d[f"grad{i}"], rtol=1e-6, atol=1e-10)
+
+
+def test_gpu_wrappers_refuse_host_tensors(tmp_path):
+    """The kernels' Python entry points raise on CPU tensors instead of passing host pointers to
+    the device."""
+    from ray_gauss_b200.filter3d import compute_3D_filter
+    from ray_gauss_b200.io import PlyVertices, write_ply
+    from ray_gauss_b200.knn import dist_cuda2
+    from ray_gauss_b200.train_tail import FusedTrainTail, LrSchedule
+    with pytest.raises(ValueError, match="CUDA"):
+        dist_cuda2(torch.zeros(8, 3))
+    with pytest.raises(ValueError, match="CUDA"):
+        compute_3D_filter(torch.zeros(8, 3), [])
+    tail = FusedTrainTail({"a": torch.zeros(4, 3)}, {"a": LrSchedule(0.1)})
+    tail.params["a"].grad = torch.ones(4, 3)
+    with pytest.raises(ValueError, match="CUDA"):
+        tail.step()
+    path = write_ply(str(tmp_path / "p"), [np.zeros((3, 3), np.float32)], ["x", "y", "z"])
+    with pytest.raises(ValueError, match="CUDA"):
+        PlyVertices(path, "cpu")
