@@ -3,7 +3,7 @@ storage, full backward to every parameter.  The backward that replays the forwar
 per-chunk hit lists must give the gradients of the backward that traverses the BVH again
 (recomputation), with an identical image.  Gradients are sums of float atomics whose order varies
 from run to run; at this size that alone moves them by about 1e-5 relative L2, so the comparison
-allows four times the difference between two replaying runs (at least 1e-5).  The record's memory
+allows four times the difference between two replaying runs, and at least 5e-5.  The record's memory
 and both backward times are recorded as test properties.
 
 FP64 finite differences run on the small scenes of test_gpu_features.py: at this size the FP64
@@ -59,7 +59,7 @@ def test_checkpointed_hit_lists_match_recomputation_at_scale(cuda, record_proper
     for k in KEYS:
         assert torch.isfinite(g1[k]).all(), k
         noise = rel_l2(g2[k].cpu().numpy(), g1[k].cpu().numpy())
-        assert rel_l2(g1[k].cpu().numpy(), g0[k].cpu().numpy()) <= max(1e-5, 4 * noise), (k, noise)
+        assert rel_l2(g1[k].cpu().numpy(), g0[k].cpu().numpy()) <= max(5e-5, 4 * noise), (k, noise)
     assert float(g0["densities"].abs().sum()) > 0
     record_property("rays", R)
     record_property("record_mb", round(4 * st1["record_words"] / 2 ** 20, 1))
