@@ -2,12 +2,16 @@
  * raygauss_b200 — C ABI of the B200 (sm_100a) engine for RayGauss's differentiable volumetric
  * Gaussian ray caster.
  *
- * Plain C: pointers, sizes and POD structs only.  Every device pointer is borrowed (the caller
- * owns it); the engine owns only its scratch (BVH, leaf records, per-view colours, gradient
- * accumulators, work counters).  Every call is ordered on the CUDA stream passed as `stream`
- * (a cudaStream_t, 0 = legacy default stream), performs no host synchronisation and no
- * allocation once the engine has been sized for the scene (rg_reserve), and returns RG_OK or
- * an RG_ERR_* code.  Device-side conditions (hit-list passes, stack overflow, watchdog,
+ * Plain C: pointers, sizes and POD structs only.  Descriptor structs (rg_gaussians, rg_settings,
+ * rg_train_tail, rg_densify, field and tensor lists ...) live in host memory; the arrays they and
+ * the arguments point to are device memory unless stated otherwise, and the kernels cannot tell a
+ * host pointer from a device one (the Python layer checks the tensors' devices; C callers must).
+ * Every device pointer is borrowed (the caller owns it); the engine owns only its scratch (BVH,
+ * leaf records, per-view colours, gradient accumulators, work counters).  Every call is ordered on
+ * the CUDA stream passed as `stream` (a cudaStream_t, 0 = legacy default stream) and returns RG_OK
+ * or an RG_ERR_* code; it performs no host synchronisation and no allocation once the engine has
+ * been sized for the scene (rg_reserve), except where an entry point says so (rg_densify_plan
+ * reads its counts back).  Device-side conditions (hit-list passes, stack overflow, watchdog,
  * non-finite input) are counted in a device status block read by rg_get_status().
  *
  * Reference interfaces replaced (paths inside the reference project):
