@@ -61,7 +61,7 @@ def densify_and_prune(tail, filter_3D: torch.Tensor, grad_threshold: float, min_
     d.split_scale_mul = float(np.float32(1.0) / np.float32(0.8 * n_split))
     d.n_split = n_split
     d.workspace = ws.data_ptr()
-    stream = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+    stream = ctypes.c_void_p(torch.cuda.current_stream(dev).cuda_stream)
     check(lib.rg_densify_plan(ctypes.byref(d), stream), None, "rg_densify_plan")
     n_out, n_sel = int(d.n_out), int(d.n_split_sel)
     normals = torch.randn((n_split * n_sel, 3), device=dev, generator=generator) if n_sel else None
@@ -99,6 +99,8 @@ def densify_and_prune(tail, filter_3D: torch.Tensor, grad_threshold: float, min_
         if v.numel() == 0:
             new_m[k].zero_()
             new_v[k].zero_()
+    for k in P:                               # leaves like the reference's concatenated tensors
+        new_p[k].requires_grad_(P[k].requires_grad)
     tail.rebind(new_p, new_m, new_v, new_stats)
     # the density prune's count (the split originals are removed by the split itself)
     n_pruned = n + int(d.n_clone) + n_split * n_sel - n_sel - n_out

@@ -317,9 +317,10 @@ class FusedTrainTail:
         return m
 
     def _launch(self, d):
-        if not self.params[self.names[0]].is_cuda:
+        dev = self.params[self.names[0]].device
+        if dev.type != "cuda":
             raise ValueError("the fused tail runs on CUDA tensors")
-        check(self.lib.rg_train_tail_step(ctypes.byref(d), ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)),
+        check(self.lib.rg_train_tail_step(ctypes.byref(d), ctypes.c_void_p(torch.cuda.current_stream(dev).cuda_stream)),
               None, "rg_train_tail_step")
 
     def step(self, min_scale: torch.Tensor | None = None, grads: dict | None = None):
