@@ -329,3 +329,24 @@ def test_gpu_wrappers_refuse_host_tensors(tmp_path):
     path = write_ply(str(tmp_path / "p"), [np.zeros((3, 3), np.float32)], ["x", "y", "z"])
     with pytest.raises(ValueError, match="CUDA"):
         PlyVertices(path, "cpu")
+
+
+def test_reference_arm_prints_the_contract_line():
+    """`bench.py --impl reference` (host cores only) prints one JSON line with the contract keys and
+    the reference-arm fields, on a tiny workload."""
+    import json
+    import subprocess
+    import sys
+    out = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), "--impl", "reference", "--n", "20000",
+                          "--views", "2", "--steps", "1", "--warmup", "3", "--cpu-rays", "16"],
+                         capture_output=True, text=True, timeout=600, cwd=ROOT)
+    assert out.returncode == 0, out.stderr[-2000:]
+    lines = [ln for ln in out.stdout.splitlines() if ln.startswith("{")]
+    assert len(lines) == 1
+    d = json.loads(lines[0])
+    for k in ("metric", "value", "unit", "n_gpus", "steps", "warmup", "ms_per_step", "higher_is_better", "scaling",
+              "vs_baseline", "dtype", "data", "config", "e2e", "cpu_baseline"):
+        assert k in d, k
+    assert d["impl"] == "reference" and d["value"] > 0 and d["unit"] == "Mrays/s"
+    assert d["e2e"]["h2d_bytes_per_step"] == 0 and d["e2e"]["d2h_bytes_per_step"] == 0
+    assert d["cpu_baseline"]["kind"] in ("reference", "port") and d["cpu_baseline"]["cores"] >= 1
