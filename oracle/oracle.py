@@ -29,11 +29,17 @@ _LIB = None
 _REF = {}
 
 
+def reference_root() -> str:
+    """The reference tree the ``ref`` build compiles from: $RAYGAUSS_REFERENCE, else /root/reference."""
+    return os.environ.get("RAYGAUSS_REFERENCE", "/root/reference")
+
+
 def build(ref: bool = False) -> None:
     """Compile liboracle.so (and, if ``ref`` and the reference tree exists, oracle/_ref)."""
     subprocess.run(["make", "-s", "-C", _HERE, "liboracle.so"], check=True)
-    if ref and os.path.isdir("/root/reference"):
-        subprocess.run(["make", "-s", "-C", _HERE, "ref"], check=True)
+    root = reference_root()
+    if ref and os.path.isdir(root):
+        subprocess.run(["make", "-s", "-C", _HERE, "ref", f"REF={root}"], check=True)
 
 
 def _lib():
@@ -45,6 +51,15 @@ def _lib():
                 build()
             _LIB = ctypes.CDLL(path)
         return _LIB
+
+
+def set_grid(on: bool) -> None:
+    """Candidate gathering through the nested-grid prefilter (default) or a scan of every Gaussian,
+    in the restatement and, when built, in the reference programs' OptiX stand-in."""
+    _lib().orc_set_grid(int(bool(on)))
+    if ref_available():
+        for stage in ("fwd", "bwd", "test"):
+            _ref(stage).ref_set_grid(int(bool(on)))
 
 
 def num_threads() -> int:

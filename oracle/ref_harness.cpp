@@ -14,6 +14,9 @@
 #include REF_SOURCE
 thread_local RgEmulRay rg_emul;
 RgEmulScene rg_emul_scene;
+/* trace calls find their primitives through the grid (1) or a per-ray scan of all AABBs (0) */
+static bool rg_use_grid = true;
+extern "C" void ref_set_grid(int on) { rg_use_grid = on != 0; }
 
 static void set_common(int n, const float* pos, const float* scl, const float* quat, const float* dens,
                        const float* rgb, const float* scene_box, const float* cam, int W, int H,
@@ -73,8 +76,9 @@ extern "C" int ref_forward(int n, const float* pos, const float* scl, const floa
     params.max_gaussians_exceeded = overflow;
     params.white_background = (unsigned)white_bg;
     g_sbt.positions = (float3*)pos; g_sbt.scales = (float3*)scl; g_sbt.quaternions = (float4*)quat;
-    rg_emul_scene.aabb = aabb; rg_emul_scene.n = n; rg_emul_scene.sbt_data = &g_sbt;
+    rg_emul_bind(aabb, n, scene_box, &g_sbt, rg_use_grid);
     run_rays(W, H, ids, n_ids);
+    rg_emul_unbind();
     std::free(hit_buf);
     return 0;
 }
@@ -97,8 +101,9 @@ extern "C" int ref_backward(int n, const float* pos, const float* scl, const flo
     params.quaternions_grad = (float4*)d_quat;
     params.handle = 0;
     g_sbt.positions = (float3*)pos; g_sbt.scales = (float3*)scl; g_sbt.quaternions = (float4*)quat;
-    rg_emul_scene.aabb = aabb; rg_emul_scene.n = n; rg_emul_scene.sbt_data = &g_sbt;
+    rg_emul_bind(aabb, n, scene_box, &g_sbt, rg_use_grid);
     run_rays(W, H, ids, n_ids);
+    rg_emul_unbind();
     std::free(hit_buf);
     return 0;
 }
@@ -106,6 +111,9 @@ extern "C" int ref_backward(int n, const float* pos, const float* scl, const flo
 #include REF_SOURCE
 thread_local RgEmulRay rg_emul;
 RgEmulScene rg_emul_scene;
+/* trace calls find their primitives through the grid (1) or a per-ray scan of all AABBs (0) */
+static bool rg_use_grid = true;
+extern "C" void ref_set_grid(int on) { rg_use_grid = on != 0; }
 static sphere::SphereHitGroupData g_sbt;
 
 /* optix_utils.py:302-373: inference launch; colours (R,3) and Gaussians per ray (R) */
@@ -140,7 +148,7 @@ extern "C" int ref_inference(int n, const float* pos, const float* scl, const fl
     params.handle = 0;
     params.white_background = (unsigned)white_bg;
     g_sbt.positions = (float3*)pos; g_sbt.scales = (float3*)scl; g_sbt.quaternions = (float4*)quat;
-    rg_emul_scene.aabb = aabb; rg_emul_scene.n = n; rg_emul_scene.sbt_data = &g_sbt;
+    rg_emul_bind(aabb, n, scene_box, &g_sbt, rg_use_grid);
     const int n_rays = ids ? n_ids : W * H;
 #pragma omp parallel for schedule(dynamic, 8)
     for (int r = 0; r < n_rays; ++r) {
@@ -149,6 +157,7 @@ extern "C" int ref_inference(int n, const float* pos, const float* scl, const fl
         rg_emul.have_cands = false;
         __raygen__rg();
     }
+    rg_emul_unbind();
     for (int r = 0; r < n_rays; ++r) {
         const int k = ids ? ids[r] : r;
         for (int c = 0; c < 3; ++c) out_colors[3 * r + c] = colors[3 * k + c];

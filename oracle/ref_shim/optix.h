@@ -6,10 +6,12 @@
  * as plain C++ on the CPU so that their own intersection, any-hit, sampling, compositing and
  * adjoint code produce reference outputs for small scenes.
  *
- * Only the traversal is emulated: optixTrace() visits every primitive of a per-ray candidate
- * list whose AABB overlaps [tmin, tmax], calls __intersection__gaussian(), and on a reported
- * intersection calls __anyhit__ah(), honouring optixTerminateRay().  OptiX itself (a closed
- * library) is not used.
+ * Only the traversal is emulated: optixTrace() visits, in primitive-index order, every primitive
+ * whose AABB overlaps [tmin, tmax], calls __intersection__gaussian(), and on a reported
+ * intersection calls __anyhit__ah(), honouring optixTerminateRay().  The primitives are found
+ * through a nested uniform grid over the AABBs (../orc_grid.h) when the scene is bound with one,
+ * else from a per-ray scan of all AABBs; both give the same primitives in the same order.  OptiX
+ * itself (a closed library) is not used.
  */
 #pragma once
 #include <vector_types.h>
@@ -18,6 +20,9 @@
 #include <vector>
 #include <cstdio>
 #include <cstring>
+#include <algorithm>
+
+#include "../orc_grid.h"
 
 typedef unsigned long long OptixTraversableHandle;
 typedef unsigned int OptixVisibilityMask;
@@ -39,12 +44,17 @@ struct RgEmulRay {
     bool terminated;
     bool have_cands;
     std::vector<int> cands;
+    std::vector<unsigned char> mark;   /* grid query scratch */
+    std::vector<int> ids;
+    std::vector<long long> key;
 };
 
 struct RgEmulScene {
     const float* aabb;  /* (n,6) lo.xyz hi.xyz */
     int n;
     void* sbt_data;
+    orc_grid* grid;     /* candidate prefilter (null: scan every AABB per ray) */
+    double* box;        /* the AABBs in double for the grid */
 };
 
 extern thread_local RgEmulRay rg_emul;
@@ -103,9 +113,60 @@ static inline bool rg_emul_box(const float* bb, float3 o, float3 d, float tmin, 
     return true;
 }
 
+/* Binds the scene of one launch: the AABBs, the hit-group record and, with use_grid, a grid over
+ * the AABBs inside the scene box. */
+static inline void rg_emul_bind(const float* aabb, int n, const float* scene_box, void* sbt, bool use_grid) {
+    rg_emul_scene.aabb = aabb;
+    rg_emul_scene.n = n;
+    rg_emul_scene.sbt_data = sbt;
+    rg_emul_scene.grid = nullptr;
+    rg_emul_scene.box = nullptr;
+    if (!use_grid || n <= 0) return;
+    rg_emul_scene.box = (double*)std::malloc(sizeof(double) * 6 * (size_t)n);
+    for (long long i = 0; i < 6 * (long long)n; ++i) rg_emul_scene.box[i] = (double)aabb[i];
+    double lo[3], hi[3];
+    for (int a = 0; a < 3; ++a) {
+        lo[a] = scene_box[a];
+        hi[a] = scene_box[3 + a];
+        if (!std::isfinite(lo[a]) || !std::isfinite(hi[a]) || !(hi[a] >= lo[a])) { lo[a] = -1.0; hi[a] = 1.0; }
+    }
+    rg_emul_scene.grid = (orc_grid*)std::malloc(sizeof(orc_grid));
+    orc_grid_build(rg_emul_scene.grid, rg_emul_scene.box, n, lo, hi);
+}
+
+static inline void rg_emul_unbind() {
+    if (rg_emul_scene.grid) {
+        orc_grid_free(rg_emul_scene.grid);
+        std::free(rg_emul_scene.grid);
+        std::free(rg_emul_scene.box);
+    }
+    rg_emul_scene.grid = nullptr;
+    rg_emul_scene.box = nullptr;
+}
+
+/* The primitives of one trace call through the grid, in index order. */
+static inline void rg_emul_grid_cands(float3 o, float3 d, float tmin, float tmax) {
+    const size_t n = (size_t)rg_emul_scene.n;
+    if (rg_emul.mark.size() < n) {
+        rg_emul.mark.assign(n, 0);
+        rg_emul.ids.resize(n);
+        rg_emul.key.resize(n);
+    }
+    double oo[3] = {o.x, o.y, o.z}, dd[3] = {d.x, d.y, d.z};
+    double t1 = std::isfinite(tmax) ? (double)tmax : 1e300;
+    double span = 1e-6 * (std::fabs((double)tmin) + std::fabs(std::isfinite(tmax) ? (double)tmax : 0.0)) + 1e-9;
+    int k = orc_grid_query(rg_emul_scene.grid, oo, dd, (double)tmin - span, t1 + span, rg_emul.mark.data(),
+                           rg_emul.ids.data());
+    orc_grid_unmark(rg_emul.mark.data(), rg_emul.ids.data(), k);
+    orc_grid_sort(rg_emul.ids.data(), k, nullptr, rg_emul.key.data());
+    rg_emul.cands.assign(rg_emul.ids.begin(), rg_emul.ids.begin() + k);
+}
+
 static inline void optixTrace(OptixTraversableHandle, float3 o, float3 d, float tmin, float tmax, float,
                               OptixVisibilityMask, unsigned, unsigned, unsigned, unsigned, unsigned& p0) {
-    if (!rg_emul.have_cands) {
+    if (rg_emul_scene.grid) {
+        rg_emul_grid_cands(o, d, tmin, tmax);
+    } else if (!rg_emul.have_cands) {
         rg_emul.cands.clear();
         for (int g = 0; g < rg_emul_scene.n; ++g)
             if (rg_emul_box(rg_emul_scene.aabb + 6 * g, o, d, 0.0f, INFINITY)) rg_emul.cands.push_back(g);

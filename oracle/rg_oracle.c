@@ -9,6 +9,11 @@
 #include <stdlib.h>
 #include <string.h>
 
+/* 1: gather ray candidates through the grid prefilter (orc_grid.h); 0: scan every Gaussian.  Both
+ * give the same candidate lists; the switch lets the tests check that. */
+static int orc_grid_enabled = 1;
+void orc_set_grid(int on) { orc_grid_enabled = on ? 1 : 0; }
+
 #define REAL float
 #define SFX _f32
 #include "rg_oracle_impl.h"

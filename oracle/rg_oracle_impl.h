@@ -25,14 +25,17 @@
  * Constants: forward/gaussians_aabb.h:2-5 (BUFFER_SIZE 8, DT 0.0025, TRANSMITTANCE_EPSILON
  * 0.003, SIGMA_THRESHOLD 0.1).  RNG: forward/gaussians_aabb.h:63-94.
  *
- * The traversal (OptiX BVH in the reference) is replaced by a brute-force candidate list per
- * ray: every Gaussian whose exact ellipsoid interval overlaps the ray's scene-box interval, in
+ * The traversal (OptiX BVH in the reference) is replaced by a candidate list per ray, prefiltered
+ * by a nested uniform grid over the AABBs (orc_grid.h) and equal to that of a scan over all
+ * Gaussians: every Gaussian whose exact ellipsoid interval overlaps the ray's scene-box interval, in
  * Gaussian index order or in a given order (e.g. a BVH leaf order, so that FP32 sums of a slab's
  * hits associate the same way as in an engine that visits hits in that order).
  * The per-slab hit decision then uses the reference's exact interval test verbatim, so the set
  * of hits per slab is the reference's set (ordered by Gaussian index; the reference's order is
  * unspecified).  Gradients are accumulated in double in both instantiations.
  */
+
+#include "orc_grid.h"
 
 #define ORC_CAT2(a, b) a##b
 #define ORC_CAT(a, b) ORC_CAT2(a, b)
@@ -280,8 +283,14 @@ void ORC_FN(orc_backward_sh)(int n, const REAL* campos, const REAL* pos, const R
 typedef struct {
     const REAL* pos; const REAL* scl; const REAL* quat; const REAL* dens; const REAL* rgb;
     int n;
+    const orc_grid* grid;   /* candidate prefilter over the AABBs */
+    const int* rank;        /* position of each Gaussian in the candidate order (NULL: index order) */
 } ORC_FN(scene_);
 #define SCENE ORC_FN(scene_)
+
+/* Per-thread scratch of the candidate gathering. */
+typedef struct { unsigned char* mark; int* ids; long long* key; } ORC_FN(gscratch_);
+#define GSCRATCH ORC_FN(gscratch_)
 
 typedef struct { int g; REAL r1, r2; } ORC_FN(cand_);
 #define CAND ORC_FN(cand_)
@@ -371,35 +380,91 @@ static inline int ORC_FN(slab_hit)(REAL lo, REAL hi, REAL r1, REAL r2) {
     return FMX(lo, r1) <= FMN(hi, r2);
 }
 
-/* All Gaussians whose exact interval overlaps [tenter, texit]; an AABB prefilter with a generous
- * margin only skips work (the exact test decides). */
+/* One candidate: an AABB prefilter with a generous margin (it only skips work), then the exact
+ * interval must overlap [tenter, texit]. */
+static int ORC_FN(cand_test)(const SCENE* S, const REAL* aabb, int g, V3 o, V3 d, V3 invd, REAL tenter, REAL texit,
+                             CAND* out) {
+    const REAL* bb = aabb + 6 * g;
+    double tn = tenter, tf = texit;
+    double oo[3] = {o.x, o.y, o.z}, id[3] = {invd.x, invd.y, invd.z};
+    for (int a = 0; a < 3; ++a) {
+        double ext = 1e-4 * (fabs((double)bb[a]) + fabs((double)bb[3 + a])) + 1e-6;
+        double lo = (double)bb[a] - ext, hi = (double)bb[3 + a] + ext;
+        double t0 = (lo - oo[a]) * id[a], t1 = (hi - oo[a]) * id[a];
+        if (isnan(t0) || isnan(t1)) continue;
+        double a0 = t0 < t1 ? t0 : t1, a1 = t0 < t1 ? t1 : t0;
+        if (a0 > tn) tn = a0;
+        if (a1 < tf) tf = a1;
+        if (tn > tf) return 0;
+    }
+    REAL r1, r2;
+    if (!ORC_FN(ellipsoid_roots)(S, g, o, d, &r1, &r2)) return 0;
+    if (!ORC_FN(slab_hit)(tenter, texit, r1, r2)) return 0;
+    out->g = g; out->r1 = r1; out->r2 = r2;
+    return 1;
+}
+
+/* All Gaussians whose exact interval overlaps [tenter, texit], in candidate order (Gaussian index,
+ * or the given order).  With a grid, only the Gaussians registered in the cells along the ray are
+ * tested, sorted back into candidate order: the list equals that of testing every Gaussian. */
 static int ORC_FN(gather_cands)(const SCENE* S, const REAL* aabb, V3 o, V3 d, REAL tenter, REAL texit,
-                                const int* order, CAND* out) {
+                                const int* order, CAND* out, GSCRATCH* gs) {
     int m = 0;
     V3 invd = MK((REAL)1 / d.x, (REAL)1 / d.y, (REAL)1 / d.z);
+    if (S->grid) {
+        double oo[3] = {o.x, o.y, o.z}, dd[3] = {d.x, d.y, d.z};
+        double span = 1e-6 * (fabs((double)tenter) + fabs((double)texit)) + 1e-9;
+        int k = orc_grid_query(S->grid, oo, dd, (double)tenter - span, (double)texit + span, gs->mark, gs->ids);
+        orc_grid_unmark(gs->mark, gs->ids, k);
+        orc_grid_sort(gs->ids, k, S->rank, gs->key);
+        for (int j = 0; j < k; ++j) m += ORC_FN(cand_test)(S, aabb, gs->ids[j], o, d, invd, tenter, texit, out + m);
+        return m;
+    }
     for (int li = 0; li < S->n; ++li) {
         int g = order ? order[li] : li;
-        const REAL* bb = aabb + 6 * g;
-        double tn = tenter, tf = texit;
-        double oo[3] = {o.x, o.y, o.z}, id[3] = {invd.x, invd.y, invd.z};
-        int miss = 0;
-        for (int a = 0; a < 3 && !miss; ++a) {
-            double ext = 1e-4 * (fabs((double)bb[a]) + fabs((double)bb[3 + a])) + 1e-6;
-            double lo = (double)bb[a] - ext, hi = (double)bb[3 + a] + ext;
-            double t0 = (lo - oo[a]) * id[a], t1 = (hi - oo[a]) * id[a];
-            if (isnan(t0) || isnan(t1)) continue;
-            double a0 = t0 < t1 ? t0 : t1, a1 = t0 < t1 ? t1 : t0;
-            if (a0 > tn) tn = a0;
-            if (a1 < tf) tf = a1;
-            if (tn > tf) miss = 1;
-        }
-        if (miss) continue;
-        REAL r1, r2;
-        if (!ORC_FN(ellipsoid_roots)(S, g, o, d, &r1, &r2)) continue;
-        if (!ORC_FN(slab_hit)(tenter, texit, r1, r2)) continue;
-        out[m].g = g; out[m].r1 = r1; out[m].r2 = r2; ++m;
+        m += ORC_FN(cand_test)(S, aabb, g, o, d, invd, tenter, texit, out + m);
     }
     return m;
+}
+
+/* Grid over the AABBs (and the rank of each Gaussian in `order`) for one render call. */
+typedef struct { orc_grid grid; double* box; int* rank; } ORC_FN(gridset_);
+#define GRIDSET ORC_FN(gridset_)
+
+static void ORC_FN(gridset_build)(GRIDSET* G, const REAL* aabb, const REAL* scene_box, int n, const int* order) {
+    memset(G, 0, sizeof(*G));
+    if (!orc_grid_enabled) return;
+    G->box = (double*)malloc(sizeof(double) * 6 * (size_t)(n > 0 ? n : 1));
+    for (long long i = 0; i < 6 * (long long)n; ++i) G->box[i] = (double)aabb[i];
+    double lo[3] = {scene_box[0], scene_box[1], scene_box[2]}, hi[3] = {scene_box[3], scene_box[4], scene_box[5]};
+    for (int a = 0; a < 3; ++a) {
+        if (!isfinite(lo[a]) || !isfinite(hi[a]) || !(hi[a] >= lo[a])) { lo[a] = -1.0; hi[a] = 1.0; }
+    }
+    orc_grid_build(&G->grid, G->box, n, lo, hi);
+    G->rank = NULL;
+    if (order) {
+        G->rank = (int*)malloc(sizeof(int) * (size_t)(n > 0 ? n : 1));
+        for (int li = 0; li < n; ++li) G->rank[order[li]] = li;
+    }
+}
+
+static void ORC_FN(gridset_free)(GRIDSET* G) {
+    if (G->box) orc_grid_free(&G->grid);
+    free(G->box);
+    free(G->rank);
+}
+
+static void ORC_FN(gscratch_alloc)(GSCRATCH* gs, int n) {
+    size_t m = (size_t)(n > 0 ? n : 1);
+    gs->mark = (unsigned char*)calloc(m, 1);
+    gs->ids = (int*)malloc(sizeof(int) * m);
+    gs->key = (long long*)malloc(sizeof(long long) * m);
+}
+
+static void ORC_FN(gscratch_free)(GSCRATCH* gs) {
+    free(gs->mark);
+    free(gs->ids);
+    free(gs->key);
 }
 
 #define ORC_BUF 8
@@ -473,13 +538,17 @@ int ORC_FN(orc_render_forward)(int n, const REAL* pos, const REAL* scl, const RE
                                int W, int H, int white_bg, int max_prim_slice, int jitter, int rnd_sample,
                                unsigned iteration, const int* ray_ids, int n_rays, const int* order, REAL* out,
                                REAL* out_T, long long* stats) {
-    SCENE S = {pos, scl, quat, dens, rgb, n};
+    GRIDSET GS;
+    ORC_FN(gridset_build)(&GS, aabb, scene_box, n, order);
+    SCENE S = {pos, scl, quat, dens, rgb, n, GS.box ? &GS.grid : NULL, GS.rank};
     long long st0 = 0, st1 = 0, st2 = 0;
     int cap = max_prim_slice > 0 ? max_prim_slice : 1024;
 #pragma omp parallel reduction(+ : st0, st1, st2)
     {
         CAND* cands = (CAND*)malloc(sizeof(CAND) * (size_t)(n > 0 ? n : 1));
         int* hits = (int*)malloc(sizeof(int) * (size_t)(n > 0 ? n : 1));
+        GSCRATCH gs;
+        ORC_FN(gscratch_alloc)(&gs, n);
 #pragma omp for schedule(dynamic, 16)
         for (int rr = 0; rr < n_rays; ++rr) {
             unsigned idx = ray_ids ? (unsigned)ray_ids[rr] : (unsigned)rr;
@@ -492,7 +561,7 @@ int ORC_FN(orc_render_forward)(int n, const REAL* pos, const REAL* scl, const RE
             REAL T = 1;
             V3 col = MK(0, 0, 0);
             if (tenter < texit) {
-                int nc = ORC_FN(gather_cands)(&S, aabb, o, d, tenter, texit, order, cands);
+                int nc = ORC_FN(gather_cands)(&S, aabb, o, d, tenter, texit, order, cands, &gs);
                 const REAL slab = ORC_DT * (REAL)ORC_BUF;
                 REAL tb = tenter;
                 while (tb < texit && T > ORC_TEPS) {
@@ -523,7 +592,9 @@ int ORC_FN(orc_render_forward)(int n, const REAL* pos, const REAL* scl, const RE
         }
         free(cands);
         free(hits);
+        ORC_FN(gscratch_free)(&gs);
     }
+    ORC_FN(gridset_free)(&GS);
     if (stats) { stats[0] = st0; stats[1] = st1; stats[2] = st2; }
     return 0;
 }
@@ -571,7 +642,9 @@ int ORC_FN(orc_render_inference)(int n, const REAL* pos, const REAL* scl, const 
                                  const REAL* rgb, const REAL* aabb, const REAL* scene_box, const REAL* cam,
                                  int W, int H, int white_bg, int max_prim_slice, int count_cap, const int* ray_ids,
                                  int n_rays, const int* order, REAL* out, int* counts, long long* stats) {
-    SCENE S = {pos, scl, quat, dens, rgb, n};
+    GRIDSET GS;
+    ORC_FN(gridset_build)(&GS, aabb, scene_box, n, order);
+    SCENE S = {pos, scl, quat, dens, rgb, n, GS.box ? &GS.grid : NULL, GS.rank};
     long long st0 = 0, st1 = 0;
     int cap = max_prim_slice > 0 ? max_prim_slice : 1024;
     int ccap = count_cap > 0 ? count_cap : cap;   /* per-slab cap of the counts alone (0: the hit cap) */
@@ -579,6 +652,8 @@ int ORC_FN(orc_render_inference)(int n, const REAL* pos, const REAL* scl, const 
     {
         CAND* cands = (CAND*)malloc(sizeof(CAND) * (size_t)(n > 0 ? n : 1));
         int* hits = (int*)malloc(sizeof(int) * (size_t)(n > 0 ? n : 1));
+        GSCRATCH gs;
+        ORC_FN(gscratch_alloc)(&gs, n);
 #pragma omp for schedule(dynamic, 16)
         for (int rr = 0; rr < n_rays; ++rr) {
             unsigned idx = ray_ids ? (unsigned)ray_ids[rr] : (unsigned)rr;
@@ -594,7 +669,7 @@ int ORC_FN(orc_render_inference)(int n, const REAL* pos, const REAL* scl, const 
             if (tenter < texit) {
                 const REAL slab = ORC_DT * (REAL)ORC_BUF;
                 /* candidates over the whole marched range: the last slab reaches past texit */
-                int nc = ORC_FN(gather_cands)(&S, aabb, o, d, tenter, texit + slab, order, cands);
+                int nc = ORC_FN(gather_cands)(&S, aabb, o, d, tenter, texit + slab, order, cands, &gs);
                 REAL tb = tenter;
                 while (tb < texit && T > ORC_TEPS) {
                     REAL lo = tb, hi = tb + slab;
@@ -624,7 +699,9 @@ int ORC_FN(orc_render_inference)(int n, const REAL* pos, const REAL* scl, const 
         }
         free(cands);
         free(hits);
+        ORC_FN(gscratch_free)(&gs);
     }
+    ORC_FN(gridset_free)(&GS);
     if (stats) { stats[0] = st0; stats[1] = st1; }
     return 0;
 }
@@ -639,13 +716,17 @@ int ORC_FN(orc_render_backward)(int n, const REAL* pos, const REAL* scl, const R
                                 const REAL* ray_colors, const REAL* dL,
                                 double* drgb, double* ddens, double* dpos, double* dscl, double* dquat,
                                 long long* stats) {
-    SCENE S = {pos, scl, quat, dens, rgb, n};
+    GRIDSET GS;
+    ORC_FN(gridset_build)(&GS, aabb, scene_box, n, order);
+    SCENE S = {pos, scl, quat, dens, rgb, n, GS.box ? &GS.grid : NULL, GS.rank};
     long long st0 = 0, st1 = 0;
     int cap = max_prim_slice > 0 ? max_prim_slice : 1024;
 #pragma omp parallel reduction(+ : st0, st1)
     {
         CAND* cands = (CAND*)malloc(sizeof(CAND) * (size_t)(n > 0 ? n : 1));
         int* hits = (int*)malloc(sizeof(int) * (size_t)(n > 0 ? n : 1));
+        GSCRATCH gs;
+        ORC_FN(gscratch_alloc)(&gs, n);
 #pragma omp for schedule(dynamic, 16)
         for (int rr = 0; rr < n_rays; ++rr) {
             unsigned idx = ray_ids ? (unsigned)ray_ids[rr] : (unsigned)rr;
@@ -655,7 +736,7 @@ int ORC_FN(orc_render_backward)(int n, const REAL* pos, const REAL* scl, const R
             REAL tenter, texit;
             ORC_FN(scene_clip)(scene_box, o, d, &tenter, &texit);
             if (!(tenter < texit)) continue;
-            int nc = ORC_FN(gather_cands)(&S, aabb, o, d, tenter, texit, order, cands);
+            int nc = ORC_FN(gather_cands)(&S, aabb, o, d, tenter, texit, order, cands, &gs);
             const REAL slab = ORC_DT * (REAL)ORC_BUF;
             REAL tb = tenter;
             REAL Tb = 1;
@@ -762,7 +843,9 @@ int ORC_FN(orc_render_backward)(int n, const REAL* pos, const REAL* scl, const R
         }
         free(cands);
         free(hits);
+        ORC_FN(gscratch_free)(&gs);
     }
+    ORC_FN(gridset_free)(&GS);
     if (stats) { stats[0] = st0; stats[1] = st1; }
     return 0;
 }
@@ -781,6 +864,8 @@ int ORC_FN(orc_render_backward)(int n, const REAL* pos, const REAL* scl, const R
 #undef FMX
 #undef SCENE
 #undef CAND
+#undef GSCRATCH
+#undef GRIDSET
 #undef GAUSS
 #undef ORC_BUF
 #undef ORC_DT

@@ -188,3 +188,75 @@ def test_oracle_inference_differs_from_training_forward_only_slightly(oracle):
     fwd, _, _ = oracle.render_forward(*args)
     d = np.abs(img - fwd).max()
     assert 0.0 < d <= 1e-3
+
+
+@pytest.mark.parametrize("workload", ["unbounded", "bounded"])
+def test_grid_prefilter_gives_the_scan_results(oracle, workload):
+    """The nested-grid candidate prefilter returns the candidate lists of a scan over every
+    Gaussian, in the same order: images, transmittances and gradients are bit-identical."""
+    from ray_gauss_b200 import synthetic as S
+    if workload == "unbounded":
+        p = S.unbounded(60_000, seed=3, nsg=0)
+        cam = S.ring_cameras(1, seed=3, w_range=(96, 96))[0]
+    else:
+        p = S.bounded_object(40_000, seed=3, nsg=0)
+        cam = S.sphere_camera(4.0, 96, 72, 40.0, seed=3)
+    P = {k: np.asarray(v, np.float32) for k, v in p.items()}
+    W, H = cam.image_width, cam.image_height
+    ids = np.random.default_rng(1).choice(W * H, 600, replace=False).astype(np.int32)
+    cv = oracle.camera_vector(cam)
+    rgb = oracle.forward_sh(cv[:3], P["positions"], P["color_features"], None, None, None)
+    dL = np.random.default_rng(2).normal(0, 1, (ids.size, 3)).astype(np.float32)
+    out = {}
+    try:
+        for on in (True, False):
+            oracle.set_grid(on)
+            img, T, st = oracle.render_forward(P["positions"], P["scales"], P["quaternions"], P["densities"], rgb, cv,
+                                               W, H, True, ray_ids=ids)
+            g = oracle.render_backward(P["positions"], P["scales"], P["quaternions"], P["densities"], rgb, cv, W, H,
+                                       img, dL, ray_ids=ids)
+            out[on] = (img, T, st, g)
+    finally:
+        oracle.set_grid(True)
+    assert out[True][2][1] > 0   # hits were found
+    assert np.array_equal(out[True][0], out[False][0]) and np.array_equal(out[True][1], out[False][1])
+    assert np.array_equal(out[True][2], out[False][2])
+    for k in ("d_rgb", "d_dens", "d_pos", "d_scl", "d_quat"):
+        assert np.array_equal(out[True][3][k], out[False][3][k]), k
+
+
+def test_reference_programs_grid_gives_the_scan_results(oracle):
+    """The reference programs' OptiX stand-in finds each trace call's primitives through the grid:
+    same primitives in the same order as its per-ray scan, so bit-identical outputs."""
+    if not oracle.ref_available():
+        pytest.skip("reference programs not built (oracle/_ref)")
+    from ray_gauss_b200 import synthetic as S
+    p = S.unbounded(20_000, seed=5, nsg=0)
+    cam = S.ring_cameras(1, seed=5, w_range=(64, 64))[0]
+    P = {k: np.asarray(v, np.float32) for k, v in p.items()}
+    W, H = cam.image_width, cam.image_height
+    ids = np.random.default_rng(3).choice(W * H, 200, replace=False).astype(np.int32)
+    cv = oracle.camera_vector(cam).astype(np.float32)
+    rgb = oracle.ref_forward_sh(cv[:3], P["positions"], P["color_features"], None, None, None)
+    dL = np.random.default_rng(4).normal(0, 1, (W * H, 3)).astype(np.float32)
+    out = {}
+    try:
+        for on in (True, False):
+            oracle.set_grid(on)
+            img, ovf = oracle.ref_render_forward(P["positions"], P["scales"], P["quaternions"], P["densities"], rgb,
+                                                 cv, W, H, True, ray_ids=ids)
+            g = oracle.ref_render_backward(P["positions"], P["scales"], P["quaternions"], P["densities"], rgb, cv,
+                                           W, H, img, dL, ray_ids=ids)
+            inf, cnt = oracle.ref_render_inference(P["positions"], P["scales"], P["quaternions"], P["densities"],
+                                                   rgb, cv, W, H, True, ray_ids=ids)
+            out[on] = (img, g, inf, cnt)
+    finally:
+        oracle.set_grid(True)
+    assert np.abs(out[True][0][ids] - 1.0).max() > 0.01   # the rays see the scene
+    assert np.array_equal(out[True][0], out[False][0])
+    # the backward programs add gradients with float atomics from OpenMP threads, whose order
+    # differs from run to run (scan against scan differs by ~3e-7 of the largest entry)
+    for k in ("d_rgb", "d_dens", "d_pos", "d_scl", "d_quat"):
+        a, b = out[True][1][k], out[False][1][k]
+        assert np.abs(a - b).max() <= 2e-6 * np.abs(b).max(), k
+    assert np.array_equal(out[True][2], out[False][2]) and np.array_equal(out[True][3], out[False][3])
