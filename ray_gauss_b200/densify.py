@@ -24,11 +24,16 @@ from ._lib import check
 
 
 def densify_and_prune(tail, filter_3D: torch.Tensor, grad_threshold: float, min_density: float, scene_extent: float,
-                      n_split: int = 2, generator: torch.Generator | None = None) -> dict:
+                      n_split: int = 2, generator: torch.Generator | None = None,
+                      normals: torch.Tensor | None = None) -> dict:
     """Densify and prune the Gaussians held by ``tail`` (a :class:`ray_gauss_b200.train_tail.FusedTrainTail`
     with the ``positions``, ``scales`` (log), ``quaternions`` and ``densities`` roles and its
     statistics).  The tail is rebound to the new tensors; returns
-    ``{"params", "filter_3D", "n_clone", "n_split", "n_pruned", "n"}``."""
+    ``{"params", "filter_3D", "n_clone", "n_split", "n_pruned", "n"}``.
+
+    ``normals`` (optional, FP32 (n_split * selected, 3)) are the standard normals of the split
+    samples, taken instead of drawing them with ``generator``: a caller that reproduces another
+    run's random stream passes them (a wrong row count raises)."""
     roles = tail.roles
     for r in ("positions", "scales", "quaternions", "densities"):
         if r not in roles:
@@ -45,6 +50,14 @@ def densify_and_prune(tail, filter_3D: torch.Tensor, grad_threshold: float, min_
     f3d = filter_3D.reshape(-1)
     if f3d.numel() != n or f3d.dtype != torch.float32 or not f3d.is_contiguous():
         raise ValueError("filter_3D: (N,) or (N, 1) FP32 contiguous")
+    # the kernels launch on the current CUDA device: make it the tensors' device for the call
+    with torch.cuda.device(dev):
+        return _densify(tail, lib, P, roles, pos, ls, quat, dens, f3d, tuple(filter_3D.shape), n, dev,
+                        grad_threshold, min_density, scene_extent, n_split, generator, normals)
+
+
+def _densify(tail, lib, P, roles, pos, ls, quat, dens, f3d, f3d_shape, n, dev, grad_threshold, min_density,
+             scene_extent, n_split, generator, normals):
     nbytes = ctypes.c_uint64()
     check(lib.rg_densify_workspace_bytes(n, n_split, ctypes.byref(nbytes)), None, "rg_densify_workspace_bytes")
     ws = torch.empty(int(nbytes.value), dtype=torch.uint8, device=dev)
@@ -64,13 +77,19 @@ def densify_and_prune(tail, filter_3D: torch.Tensor, grad_threshold: float, min_
     stream = ctypes.c_void_p(torch.cuda.current_stream(dev).cuda_stream)
     check(lib.rg_densify_plan(ctypes.byref(d), stream), None, "rg_densify_plan")
     n_out, n_sel = int(d.n_out), int(d.n_split_sel)
-    normals = torch.randn((n_split * n_sel, 3), device=dev, generator=generator) if n_sel else None
+    if normals is None:
+        normals = torch.randn((n_split * n_sel, 3), device=dev, generator=generator) if n_sel else None
+    else:
+        if normals.shape != (n_split * n_sel, 3):
+            raise ValueError(f"normals: expected ({n_split * n_sel}, 3) for {n_sel} split Gaussians, got "
+                             f"{tuple(normals.shape)}")
+        normals = normals.to(device=dev, dtype=torch.float32).contiguous() if n_sel else None
 
     new_p = {k: torch.empty((n_out,) + tuple(v.shape[1:]), dtype=v.dtype, device=dev) for k, v in P.items()}
     new_m = {k: torch.empty_like(new_p[k]) for k in P}
     new_v = {k: torch.empty_like(new_p[k]) for k in P}
     new_stats = {k: torch.empty(n_out, dtype=torch.float32, device=dev) for k in tail.stats}
-    new_f3d = torch.empty((n_out,) + tuple(filter_3D.shape[1:]), dtype=torch.float32, device=dev)
+    new_f3d = torch.empty((n_out,) + tuple(f3d_shape[1:]), dtype=torch.float32, device=dev)
     kind_of = {roles["positions"]: _lib.RG_DENSIFY_POSITIONS, roles["scales"]: _lib.RG_DENSIFY_LOG_SCALES,
                roles["densities"]: _lib.RG_DENSIFY_DENSITIES}
     items = []

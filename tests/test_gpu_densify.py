@@ -1,10 +1,14 @@
-"""Densify and prune against the reference's densify_and_prune restated in torch
-(classes/point_cloud.py:497-516, 1037-1143; the optimizer-state surgery of classes/optimizer.py:54-83;
-build_rotation of utils/general_utils.py:466-487), on the same random normals.
+"""Densify and prune against the reference's own densify_and_prune and optimizer-state surgery
+(classes/point_cloud.py:497-516, 1034-1143; classes/optimizer.py:54-83, 151-164): fixtures that
+tests/golden/make_densify_golden.py generates by running those functions on the CPU, fed with the
+same standard normals; and, at sizes a fixture cannot hold (1.1M Gaussians), against the same
+functions restated in torch (_RefCloud; build_rotation of utils/general_utils.py:466-487).
 
 Every tensor must match row for row: exactly, except the positions and log scales of split copies
 (a 3x3 product and a division by a Python number whose operation order inside torch is not
-specified) within 1e-6 relative + 1e-6 absolute."""
+specified, and the CPU's exponential against the GPU's) within 1e-6 relative + 1e-6 absolute."""
+import os
+
 import numpy as np
 import pytest
 import torch
@@ -245,3 +249,50 @@ def test_densify_with_zero_width_sg_tensors_in_the_tail(cuda):
     tail.step(min_scale=out["filter_3D"])
     torch.cuda.synchronize()
     assert all(torch.isfinite(x).all() for x in tail.params.values())
+
+
+@pytest.mark.parametrize("case", ["mixed", "sg8_extent"])
+def test_densify_matches_the_reference_functions(cuda, case):
+    """Inputs, normals and outputs of the reference's PointCloud.densify_and_prune with its Adam
+    optimizers (three real steps taken before), including rows whose mean gradient is infinite."""
+    from conftest import GOLDEN
+    from ray_gauss_b200.densify import densify_and_prune
+    from ray_gauss_b200.train_tail import FusedTrainTail, LrSchedule
+    z = np.load(os.path.join(GOLDEN, "densify", case + ".npz"))
+    t = lambda a: torch.tensor(np.ascontiguousarray(a), device=cuda)  # noqa: E731
+    tail = FusedTrainTail({k: t(z[f"in/{k}"]) for k in NAMES}, {k: LrSchedule(1e-3) for k in NAMES}, roles=ROLES)
+    tail.adam_step = {k: int(z[f"in_step/{k}"]) for k in NAMES}
+    for k in NAMES:
+        tail.exp_avg[k].copy_(t(z[f"in_m/{k}"]))
+        tail.exp_avg_sq[k].copy_(t(z[f"in_v/{k}"]))
+    for k in tail.stats:
+        tail.stats[k].copy_(t(z[f"in_stat/{k}"]))
+    out = densify_and_prune(tail, t(z["in_filter_3D"]), float(z["max_grad"]), float(z["min_density"]),
+                            float(z["extent"]), n_split=int(z["n_split"]), normals=t(z["normals"]))
+    torch.cuda.synchronize()
+    n_out = z["out/positions"].shape[0]
+    assert out["n"] == n_out and out["n_split"] * int(z["n_split"]) == z["normals"].shape[0]
+    for k in NAMES:
+        a, b = tail.params[k], t(z[f"out/{k}"])
+        assert a.shape == b.shape, k
+        if k in ("positions", "scales"):
+            assert torch.allclose(a, b, rtol=1e-6, atol=1e-6), (k, (a - b).abs().max().item())
+        else:
+            assert torch.equal(a, b), k
+        assert torch.equal(tail.exp_avg[k], t(z[f"out_m/{k}"])), k
+        assert torch.equal(tail.exp_avg_sq[k], t(z[f"out_v/{k}"])), k
+        assert int(tail.adam_step[k]) == int(z[f"out_step/{k}"]), k
+    for k in tail.stats:
+        assert torch.equal(tail.stats[k], t(z[f"out_stat/{k}"])), k
+    assert torch.equal(out["filter_3D"], t(z["out_filter_3D"]))
+
+
+def test_densify_rejects_normals_of_the_wrong_size(cuda):
+    from ray_gauss_b200.densify import densify_and_prune
+    from ray_gauss_b200.train_tail import FusedTrainTail, LrSchedule
+    raw, m, v, stats, f3d = _cloud(3000, cuda, seed=5)
+    tail = FusedTrainTail({k: raw[k].clone() for k in NAMES}, {k: LrSchedule(1e-3) for k in NAMES}, roles=ROLES)
+    for k in stats:
+        tail.stats[k].copy_(stats[k])
+    with pytest.raises(ValueError, match="normals"):
+        densify_and_prune(tail, f3d.clone(), 1e-4, 0.1, 1.0, normals=torch.zeros((1, 3), device=cuda))
