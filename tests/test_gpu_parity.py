@@ -1,8 +1,13 @@
 """Parity of the sm_100a engine with the reference (golden fixtures) and with the CPU oracle.
 
 Tolerances: the drop-in (mode "parity", FP32) must match the reference with image max-abs <= 1e-4
-and gradient relative L2 <= 1e-3; the fast mode is held to max-abs <= 1e-3 / rel-L2 <= 1e-2 against
-the reference and reports PSNR against the FP64 oracle.
+and gradient relative L2 <= 1e-3.  The fast arithmetic (the batched form's) is held to the same
+gradient bar, 1e-3 relative L2 against the reference's arithmetic, with FP32 storage and with the
+densities, SH and SG amplitudes stored in BF16 (then against the reference's arithmetic on the
+BF16-rounded parameters, the gradients read as the engine's FP32 outputs); its images must stay
+within 1e-4 of the golden references and 5e-4 of the FP32 oracle on the 10k scene (a sample on the
+other side of the 0.1 density threshold moves a pixel by up to ~2.5e-4), and at >= 60 dB PSNR
+against the FP64 oracle.
 """
 import numpy as np
 import pytest
@@ -15,6 +20,9 @@ pytestmark = pytest.mark.gpu
 
 IMG_TOL = 1e-4
 GRAD_TOL = 1e-3
+BF16_KEYS = ("densities", "color_features", "sph_gauss_features")
+KEYS = ("positions", "scales", "quaternions", "densities", "color_features", "sph_gauss_features",
+        "bandwidth_sharpness", "lobe_axis")
 
 
 def _params(c, dev, grad=True):
@@ -64,10 +72,10 @@ def test_parity_mode_matches_reference(cuda, name):
 def test_fast_mode_close_to_reference(cuda, oracle, name):
     c = load_golden(name)
     img, g = _run_golden(c, cuda, "fast")
-    assert np.abs(img - c["ref_image"]).max() <= 1e-3
+    assert np.abs(img - c["ref_image"]).max() <= IMG_TOL
     keys = GRAD_KEYS + (SG_KEYS if c["in_sph_gauss_features"].shape[2] else [])
     for k, ref in keys:
-        assert rel_l2(g[k], c[ref]) <= 1e-2, (k, rel_l2(g[k], c[ref]))
+        assert rel_l2(g[k], c[ref]) <= GRAD_TOL, (k, rel_l2(g[k], c[ref]))
     P = {k[3:]: c[k] for k in c if k.startswith("in_")}
     img64, _, _ = oracle.render_forward(P["positions"], P["scales"], P["quaternions"], P["densities"], c["ref_rgb"],
                                         c["cam"], int(c["width"]), int(c["height"]), bool(c["white"]), prec="f64")
@@ -97,11 +105,11 @@ def test_small_object_full_size_against_oracle(cuda, oracle, mode):
     ref, _, _ = oracle.render_forward(Pn["positions"], Pn["scales"], Pn["quaternions"], Pn["densities"], rgb, cv, 200,
                                       200, white)
     out = img.detach().cpu().numpy()
-    tol = IMG_TOL if mode == "parity" else 1e-3
+    tol = IMG_TOL if mode == "parity" else 5e-4
     assert np.abs(out - ref).max() <= tol
     g = oracle.render_backward(Pn["positions"], Pn["scales"], Pn["quaternions"], Pn["densities"], rgb, cv, 200, 200,
                                ref, dL.cpu().numpy())
-    gtol = GRAD_TOL if mode == "parity" else 1e-2
+    gtol = GRAD_TOL
     assert rel_l2(P["densities"].grad.cpu().numpy(), g["d_dens"]) <= gtol
     assert rel_l2(P["scales"].grad.cpu().numpy(), g["d_scl"]) <= gtol
     assert rel_l2(P["quaternions"].grad.cpu().numpy(), g["d_quat"]) <= gtol
@@ -264,3 +272,72 @@ def test_render_is_deterministic_in_forward(cuda):
     a = _render(P, cam)
     b = _render(P, cam)
     assert torch.equal(a, b)
+
+
+def _engine_view(P, cam, mode, white, dL, bf16):
+    """Image and FP32 gradients of one view through the engine's entry points (the gradients of
+    BF16-stored tensors as the kernels write them, before any cast to the tensor's dtype)."""
+    from ray_gauss_b200 import _lib
+    from ray_gauss_b200.engine import Engine, make_gaussians, settings_struct
+    dev = P["positions"].device
+    T = dict(P)
+    if bf16:
+        for k in BF16_KEYS:
+            T[k] = T[k].to(torch.bfloat16)
+    eng = Engine(dev.index or 0)
+    g = make_gaussians(*(T[k] for k in KEYS))
+    cams_t, recs, _ = eng.cameras([cam])
+    st = settings_struct(white, mode=_lib.RG_MODE_FAST if mode == "fast" else _lib.RG_MODE_PARITY)
+    out, _ = eng.render_forward(g, cams_t, 1, recs[0].width * recs[0].height, st)
+    gr = eng.render_backward(g, cams_t, 1, st, out, dL)
+    torch.cuda.synchronize()
+    return out.cpu().numpy(), {k: v.cpu().numpy() for k, v in gr.items()}
+
+
+def _oracle_grads(oracle, P, cv, W, H, white, dL):
+    nsg = P["sph_gauss_features"].shape[2]
+    sg, kap, ax = ((P["sph_gauss_features"], P["bandwidth_sharpness"], P["lobe_axis"]) if nsg else (None,) * 3)
+    rgb = oracle.forward_sh(cv[:3], P["positions"], P["color_features"], sg, kap, ax)
+    img, _, _ = oracle.render_forward(P["positions"], P["scales"], P["quaternions"], P["densities"], rgb, cv, W, H,
+                                      white)
+    g = oracle.render_backward(P["positions"], P["scales"], P["quaternions"], P["densities"], rgb, cv, W, H, img, dL)
+    dsh, dpos, dsg, dkap, dax = oracle.backward_sh(cv[:3], P["positions"], P["color_features"], sg, kap, ax,
+                                                   g["d_rgb"].astype(np.float32))
+    out = dict(positions=g["d_pos"] + dpos, scales=g["d_scl"], quaternions=g["d_quat"], densities=g["d_dens"],
+               color_features=dsh)
+    if nsg:
+        out.update(sph_gauss_features=dsg, bandwidth_sharpness=dkap, lobe_axis=dax)
+    return img, out
+
+
+def _rounded(P):
+    return {k: (v.to(torch.bfloat16).float() if k in BF16_KEYS else v).cpu().numpy() for k, v in P.items()}
+
+
+@pytest.mark.parametrize("name", ["small_object_sh3", "shells_sg8", "inside_camera"])
+def test_fast_mode_bf16_storage_golden_scenes(cuda, oracle, name):
+    """BF16-stored densities, SH and SG amplitudes in the fast arithmetic against the reference's
+    arithmetic (FP32 oracle, pinned to the reference's programs) on the BF16-rounded parameters."""
+    c = load_golden(name)
+    P = {k[3:]: torch.tensor(c[k], dtype=torch.float32, device=cuda) for k in c if k.startswith("in_")}
+    cam = camera_from_vector(c["cam"], int(c["width"]), int(c["height"]), cuda)
+    W, H, white = int(c["width"]), int(c["height"]), bool(c["white"])
+    img, g = _engine_view(P, cam, "fast", white, torch.tensor(c["dL"], device=cuda), True)
+    ref_img, ref_g = _oracle_grads(oracle, _rounded(P), c["cam"], W, H, white, c["dL"])
+    assert np.abs(img - ref_img).max() <= IMG_TOL
+    for k, v in ref_g.items():
+        assert rel_l2(g[k], v) <= GRAD_TOL, (k, rel_l2(g[k], v))
+
+
+def test_fast_mode_bf16_storage_small_object_full_size(cuda, oracle):
+    """The 10k-Gaussian, 200x200 workload with BF16 storage in the fast arithmetic."""
+    P, cam, white = _config1(cuda)
+    P = {k: v.detach() for k, v in P.items()}
+    rng = np.random.default_rng(5)
+    dL = rng.normal(0, 1e-4, (200 * 200, 3)).astype(np.float32)
+    img, g = _engine_view(P, cam, "fast", white, torch.tensor(dL, device=cuda), True)
+    cv = oracle.camera_vector(cam)
+    ref_img, ref_g = _oracle_grads(oracle, _rounded(P), cv, 200, 200, white, dL)
+    assert np.abs(img - ref_img).max() <= 5e-4
+    for k, v in ref_g.items():
+        assert rel_l2(g[k], v) <= GRAD_TOL, (k, rel_l2(g[k], v))

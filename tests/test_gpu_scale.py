@@ -6,9 +6,16 @@ from run to run; at this size that alone moves them by about 1e-5 relative L2, s
 allows four times the difference between two replaying runs, and at least 5e-5.  The record's memory
 and both backward times are recorded as test properties.
 
-FP64 finite differences run on the small scenes of test_gpu_features.py: at this size the FP64
-oracle cannot render on the host, and FP32 differences include the jumps of samples crossing the
-density threshold, which the adjoint (like the reference's) does not differentiate."""
+The same scene is held to the oracle on seeded rays: with the loss gradient non-zero on 128 rays
+of each view, the parameter gradients are sums over those rays, which the oracle computes on the
+host.  Both backward forms (replayed hit lists and recomputation) and both arithmetics must give
+every gradient within 1e-3 relative L2 and the image of those rays within 1e-4 (parity) or 5e-4
+(fast arithmetic, whose samples can fall on the other side of the density threshold).
+
+FP64 finite differences run on the small scenes of test_gpu_features.py: FP32 differences at this
+size include the jumps of samples crossing the density threshold, which the adjoint (like the
+reference's) does not differentiate."""
+import numpy as np
 import pytest
 import torch
 
@@ -68,3 +75,59 @@ def test_checkpointed_hit_lists_match_recomputation_at_scale(cuda, record_proper
     record_property("backward_recompute_ms", round(b0, 1))
     print(f"3M x 4x1080p: forward {f1:.1f} ms, backward replaying {b1:.1f} ms, recomputing {b0:.1f} ms, "
           f"record {4 * st1['record_words'] / 2 ** 20:.1f} MB")
+
+
+@pytest.mark.parametrize("mode", ["fast", "parity"])
+def test_scale_gradients_against_oracle_on_seeded_rays(cuda, oracle, mode):
+    from ray_gauss_b200 import synthetic as S
+    from ray_gauss_b200.batched import BatchedRenderFunction, BatchedViews
+    from ray_gauss_b200.engine import Engine
+    p, cams, white = S.workload("unbounded_3m", seed=0, device="cpu")
+    P = {k: v.to(cuda).contiguous() for k, v in p.items()}
+    cams = [c.to(cuda) for c in cams]
+    eng = Engine(cuda.index or 0)
+    views = BatchedViews(cams, engine=eng, mode=mode, white_background=white)
+    R = views.n_rays
+    eng.reserve(P["positions"].shape[0], len(cams), R)
+    rng = np.random.default_rng(31)
+    ids = [np.sort(rng.choice(1920 * 1080, 128, replace=False)).astype(np.int32) for _ in cams]
+    dls = [rng.normal(0.0, 1e-3, (128, 3)).astype(np.float32) for _ in cams]
+    dL = torch.zeros((R, 3), device=cuda)
+    for v in range(len(cams)):
+        dL[torch.from_numpy(ids[v].astype(np.int64) + int(views.offsets[v])).to(cuda)] = torch.from_numpy(dls[v]).to(cuda)
+    Pn = {k: v.numpy().astype(np.float32) for k, v in p.items()}
+    ref_img, ref_g = [], {k: 0.0 for k in KEYS}
+    for v, cam in enumerate(cams):
+        cv = oracle.camera_vector(cam)
+        rgb = oracle.forward_sh(cv[:3], Pn["positions"], Pn["color_features"], Pn["sph_gauss_features"],
+                                Pn["bandwidth_sharpness"], Pn["lobe_axis"])
+        aabb, box = oracle.bbox(Pn["positions"], Pn["scales"], Pn["quaternions"], Pn["densities"])
+        img, _, _ = oracle.render_forward(Pn["positions"], Pn["scales"], Pn["quaternions"], Pn["densities"], rgb, cv,
+                                          1920, 1080, white, ray_ids=ids[v], aabb=aabb, scene_box=box)
+        g = oracle.render_backward(Pn["positions"], Pn["scales"], Pn["quaternions"], Pn["densities"], rgb, cv, 1920,
+                                   1080, img, dls[v], ray_ids=ids[v], aabb=aabb, scene_box=box)
+        dsh, dpos, dsg, dkap, dax = oracle.backward_sh(cv[:3], Pn["positions"], Pn["color_features"],
+                                                       Pn["sph_gauss_features"], Pn["bandwidth_sharpness"],
+                                                       Pn["lobe_axis"], g["d_rgb"].astype(np.float32))
+        gv = dict(positions=g["d_pos"] + dpos, scales=g["d_scl"], quaternions=g["d_quat"], densities=g["d_dens"],
+                  color_features=dsh, sph_gauss_features=dsg, bandwidth_sharpness=dkap, lobe_axis=dax)
+        for k in KEYS:
+            ref_g[k] = ref_g[k] + gv[k]
+        ref_img.append(img)
+    for record in (True, False):
+        eng.set_tuning(record_hits=1 if record else -1)
+        Q = {k: v.detach().clone().requires_grad_(True) for k, v in P.items()}
+        eng.status(reset=True)
+        out = BatchedRenderFunction.apply(*(Q[k] for k in KEYS), views)
+        out.backward(dL)
+        torch.cuda.synchronize()
+        st = eng.status(reset=True)
+        assert (st["replayed_chunks"] > 0) == record
+        o = out.detach().cpu().numpy()
+        tol = 1e-4 if mode == "parity" else 5e-4   # fast: threshold-flip of a sample, up to ~2.5e-4
+        for v in range(len(cams)):
+            assert np.abs(o[int(views.offsets[v]) + ids[v]] - ref_img[v]).max() <= tol, (record, v)
+        for k in KEYS:
+            e = rel_l2(Q[k].grad.cpu().numpy(), ref_g[k])
+            assert e <= 1e-3, (mode, record, k, e)
+    eng.set_tuning(record_hits=1)
