@@ -23,8 +23,10 @@ def _ptr(t):
     return ctypes.c_void_p(t.data_ptr()) if t is not None else None
 
 
-def _stream():
-    return ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+def _stream(device):
+    """torch's current stream on ``device`` (the engine entry points make the engine's device
+    current for the call and restore the caller's device afterwards)."""
+    return ctypes.c_void_p(torch.cuda.current_stream(device).cuda_stream)
 
 
 @dataclass
@@ -182,12 +184,12 @@ class Engine:
 
     def status(self, reset=False):
         st = _lib.rg_status()
-        check(self.lib.rg_get_status(self.h, ctypes.byref(st), int(bool(reset)), _stream()), self.h, "rg_get_status")
+        check(self.lib.rg_get_status(self.h, ctypes.byref(st), int(bool(reset)), _stream(self.device)), self.h, "rg_get_status")
         return {k: int(getattr(st, k)) for k, _ in _lib.rg_status._fields_}
 
     def leaf_order(self, n):
         out = torch.empty((n,), dtype=torch.int32, device=self.device)
-        check(self.lib.rg_leaf_order(self.h, _ptr(out), _stream()), self.h, "rg_leaf_order")
+        check(self.lib.rg_leaf_order(self.h, _ptr(out), _stream(self.device)), self.h, "rg_leaf_order")
         return out
 
     def kernel_launches(self) -> int:
@@ -214,30 +216,30 @@ class Engine:
     # -- the C-ABI steps ----------------------------------------------------------------------------
     def ellipsoids_bbox(self, g: GaussianBatch, aabb_out=None, scene_box_out=None):
         check(self.lib.rg_ellipsoids_bbox(self.h, ctypes.byref(g.struct), _ptr(aabb_out), _ptr(scene_box_out),
-                                          _stream()), self.h, "rg_ellipsoids_bbox")
+                                          _stream(self.device)), self.h, "rg_ellipsoids_bbox")
 
     def bvh_build(self):
-        check(self.lib.rg_bvh_build(self.h, _stream()), self.h, "rg_bvh_build")
+        check(self.lib.rg_bvh_build(self.h, _stream(self.device)), self.h, "rg_bvh_build")
         self.generation += 1
 
     def bvh_refit(self):
-        check(self.lib.rg_bvh_refit(self.h, _stream()), self.h, "rg_bvh_refit")
+        check(self.lib.rg_bvh_refit(self.h, _stream(self.device)), self.h, "rg_bvh_refit")
         self.generation += 1
 
     def forward_sh(self, g: GaussianBatch, cams_t, n_cams, rgb_out=None):
         check(self.lib.rg_forward_sh(self.h, ctypes.byref(g.struct), _ptr(cams_t), int(n_cams), _ptr(rgb_out),
-                                     _stream()), self.h, "rg_forward_sh")
+                                     _stream(self.device)), self.h, "rg_forward_sh")
         self.generation += 1
 
     def launch_forward(self, cams_t, n_cams, settings, ray_colors, final_T=None):
         with self._timed("launch_forward"):
                 check(self.lib.rg_launch_forward(self.h, _ptr(cams_t), int(n_cams), ctypes.byref(settings),
-                                             _ptr(ray_colors), _ptr(final_T), _stream()), self.h, "rg_launch_forward")
+                                             _ptr(ray_colors), _ptr(final_T), _stream(self.device)), self.h, "rg_launch_forward")
 
     def launch_backward(self, cams_t, n_cams, settings, ray_colors, dL):
         with self._timed("launch_backward"):
             check(self.lib.rg_launch_backward(self.h, _ptr(cams_t), int(n_cams), ctypes.byref(settings),
-                                              _ptr(ray_colors), _ptr(dL), _stream()), self.h, "rg_launch_backward")
+                                              _ptr(ray_colors), _ptr(dL), _stream(self.device)), self.h, "rg_launch_backward")
 
     def backward_sh(self, g: GaussianBatch, cams_t, n_cams, settings, grads: dict):
         s = _lib.rg_gradients()
@@ -246,7 +248,7 @@ class Engine:
             t = grads.get(k)
             setattr(s, k, t.data_ptr() if t is not None else None)
         check(self.lib.rg_backward_sh(self.h, ctypes.byref(g.struct), _ptr(cams_t), int(n_cams), ctypes.byref(settings),
-                                      ctypes.byref(s), _stream()), self.h, "rg_backward_sh")
+                                      ctypes.byref(s), _stream(self.device)), self.h, "rg_backward_sh")
 
     # -- composite steps (RenderOptixFunction forward/backward) --------------------------------------
     def render_forward(self, g: GaussianBatch, cams_t, n_cams, n_rays, settings, refit=False, final_T=False,
@@ -269,7 +271,7 @@ class Engine:
     def launch_inference(self, cams_t, n_cams, settings, ray_colors, counts=None):
         with self._timed("launch_inference"):
             check(self.lib.rg_launch_inference(self.h, _ptr(cams_t), int(n_cams), ctypes.byref(settings),
-                                               _ptr(ray_colors), _ptr(counts), _stream()), self.h,
+                                               _ptr(ray_colors), _ptr(counts), _stream(self.device)), self.h,
                   "rg_launch_inference")
 
     def render_inference(self, g: GaussianBatch, cams_t, n_cams, n_rays, settings, refit=False, counts=False):
@@ -311,7 +313,7 @@ class Engine:
         self.launch_backward(cams_t, n_cams, settings, ray_colors, dL)
         with self._timed("backward_sh"):
             check(self.lib.rg_backward_sh(self.h, ctypes.byref(g.struct), _ptr(cams_t), int(n_cams),
-                                          ctypes.byref(settings), ctypes.byref(s), _stream()), self.h, "rg_backward_sh")
+                                          ctypes.byref(settings), ctypes.byref(s), _stream(self.device)), self.h, "rg_backward_sh")
         return grads
 
 

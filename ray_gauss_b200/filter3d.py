@@ -61,7 +61,9 @@ def compute_3D_filter(positions: torch.Tensor, cameras) -> torch.Tensor:
     mx = torch.empty(1, dtype=torch.int32, device=dev)
     out = torch.empty((n, 1), dtype=torch.float32, device=dev)
     lib = _lib.load()
-    check(lib.rg_compute_3d_filter(positions.data_ptr(), n, cams.data_ptr(), len(table), inv_focal, depth.data_ptr(),
-                                   mx.data_ptr(), out.data_ptr(), ctypes.c_void_p(torch.cuda.current_stream(dev).cuda_stream)),
-          None, "rg_compute_3d_filter")
+    with torch.cuda.device(dev):   # the kernels launch on the current CUDA device
+        check(lib.rg_compute_3d_filter(positions.data_ptr(), n, cams.data_ptr(), len(table), inv_focal,
+                                       depth.data_ptr(), mx.data_ptr(), out.data_ptr(),
+                                       ctypes.c_void_p(torch.cuda.current_stream(dev).cuda_stream)),
+              None, "rg_compute_3d_filter")
     return out

@@ -160,9 +160,10 @@ class PlyVertices:
             if affine is not None:
                 f.affine = 1
                 f.div, f.add, f.mul_a, f.mul_b = (float(x) for x in affine)
-        check(self.lib.rg_records_to_columns(self.records.data_ptr(), h.n, h.record_bytes, arr, len(targets),
-                                             ctypes.c_void_p(torch.cuda.current_stream(self.device).cuda_stream)),
-              None, "rg_records_to_columns")
+        with torch.cuda.device(self.device):   # the kernel launches on the current CUDA device
+            check(self.lib.rg_records_to_columns(self.records.data_ptr(), h.n, h.record_bytes, arr, len(targets),
+                                                 ctypes.c_void_p(torch.cuda.current_stream(self.device).cuda_stream)),
+                  None, "rg_records_to_columns")
 
     def columns(self, names, affine=None) -> torch.Tensor:
         out = torch.empty((self.n, len(names)), dtype=torch.float32, device=self.device)

@@ -25,9 +25,10 @@ def dist_cuda2(points: torch.Tensor) -> torch.Tensor:
     check(lib.rg_knn_workspace_bytes(n, ctypes.byref(nb)), None, "rg_knn_workspace_bytes")
     ws = torch.empty(int(nb.value), dtype=torch.uint8, device=points.device)
     out = torch.empty(n, dtype=torch.float32, device=points.device)
-    check(lib.rg_knn_mean_dist(points.data_ptr(), n, out.data_ptr(), ws.data_ptr(),
-                               ctypes.c_void_p(torch.cuda.current_stream(points.device).cuda_stream)),
-          None, "rg_knn_mean_dist")
+    with torch.cuda.device(points.device):   # the kernels launch on the current CUDA device
+        check(lib.rg_knn_mean_dist(points.data_ptr(), n, out.data_ptr(), ws.data_ptr(),
+                                   ctypes.c_void_p(torch.cuda.current_stream(points.device).cuda_stream)),
+              None, "rg_knn_mean_dist")
     return out
 
 

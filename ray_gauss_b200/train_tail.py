@@ -320,8 +320,9 @@ class FusedTrainTail:
         dev = self.params[self.names[0]].device
         if dev.type != "cuda":
             raise ValueError("the fused tail runs on CUDA tensors")
-        check(self.lib.rg_train_tail_step(ctypes.byref(d), ctypes.c_void_p(torch.cuda.current_stream(dev).cuda_stream)),
-              None, "rg_train_tail_step")
+        with torch.cuda.device(dev):   # the kernel launches on the current CUDA device
+            check(self.lib.rg_train_tail_step(ctypes.byref(d), ctypes.c_void_p(torch.cuda.current_stream(dev).cuda_stream)),
+                  None, "rg_train_tail_step")
 
     def step(self, min_scale: torch.Tensor | None = None, grads: dict | None = None):
         """One tail step on the current stream.  ``grads`` maps names to gradients (default: each

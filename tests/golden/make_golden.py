@@ -1,6 +1,6 @@
 """Generate the golden fixtures in tests/golden/ from the reference's own code.
 
-Run in a container where the reference tree is mounted at /root/reference:
+Run in a container where the reference tree is mounted at /root/reference (or at $RAYGAUSS_REFERENCE):
     python tests/golden/make_golden.py                     (all fixtures)
     python tests/golden/make_golden.py --inference-only    (the infer_*.npz fixtures only)
 It (1) builds oracle/_ref/ — the reference's training device programs
@@ -21,7 +21,7 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 REPO = os.path.dirname(os.path.dirname(HERE))
-REF = "/root/reference"
+REF = os.environ.get("RAYGAUSS_REFERENCE", "/root/reference")
 sys.path.insert(0, REPO)
 
 from oracle import oracle as O  # noqa: E402
@@ -149,7 +149,7 @@ def sh_twin_case():
 
 
 def main():
-    subprocess.run(["make", "-s", "-C", os.path.join(REPO, "oracle"), "all", "ref"], check=True)
+    subprocess.run(["make", "-s", "-C", os.path.join(REPO, "oracle"), "all", "ref", f"REF={REF}"], check=True)
     if "--inference-only" in sys.argv:
         inference_cases()
         return

@@ -1,6 +1,6 @@
 """Generate tests/golden/loss/loss_l1_ssim.npz with the reference's own loss functions.
 
-Run in a container where the reference tree is mounted at /root/reference:
+Run in a container where the reference tree is mounted at /root/reference (or at $RAYGAUSS_REFERENCE):
     python tests/golden/make_loss_golden.py
 utils/loss_utils.py (torch only) computes l1_loss, ssim and the training loss of
 scripts/train.py:110-112, (1 - 0.2) L1 + 0.2 (1 - SSIM), with its gradient with respect to the

@@ -1,6 +1,6 @@
 """Generate the PLY fixtures in tests/golden/ply/ with the reference's own PLY module.
 
-Run in a container where the reference tree is mounted at /root/reference:
+Run in a container where the reference tree is mounted at /root/reference (or at $RAYGAUSS_REFERENCE):
     python tests/golden/make_ply_golden.py
 The reference's scripts/ply.py (numpy only) writes the point-cloud files and reads them back; the
 fixtures hold the files and, in expected.npz, every field as the reference's read_ply returns it
