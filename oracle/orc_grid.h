@@ -5,8 +5,8 @@
  *
  * The top level covers the scene box with res^3 cells (res ~ cbrt(n / 8), at most 96 per axis).
  * A cell that receives more than ORC_GRID_LEAF boxes, whose boxes are on average small against its
- * children (mean largest extent below two child cells), and that lies less than ORC_GRID_DEPTH levels
- * down is split into 8^3 child cells; otherwise it keeps its list of boxes.  Unbounded scenes (most
+ * children (mean largest extent below four child cells), and that lies less than ORC_GRID_DEPTH
+ * levels down is split into 8^3 child cells; otherwise it keeps its list of boxes.  Unbounded scenes (most
  * Gaussians in a small core, a sparse far field) thereby get fine cells only where they are dense.
  *
  * A query walks the cells that the segment o + t d, t in [t0, t1], passes through (3-D DDA in
@@ -94,11 +94,7 @@ static void orc_grid_level_build(orc_grid* G, const int* items, int m, const dou
     L.cell0 = G->n_cells;
     const long long nc = (long long)res * res * res;
     G->first = (long long*)orc_grid_grow(G->first, &G->cap_cells, G->n_cells + nc, sizeof(long long));
-    {
-        long long cap = G->cap_cells;   /* count grows with the same capacity sequence */
-        (void)cap;
-    }
-    G->count = (int*)realloc(G->count, (size_t)G->cap_cells * sizeof(int));
+    G->count = (int*)realloc(G->count, (size_t)G->cap_cells * sizeof(int));   /* same capacity as first */
     G->n_cells += nc;
     G->lv[li] = L;
     /* count boxes per cell and their mean largest extent */
@@ -139,7 +135,7 @@ static void orc_grid_level_build(orc_grid* G, const int* items, int m, const dou
     for (long long c = 0; c < nc; ++c) {
         const long long gc = L.cell0 + c;
         const int n_in = cnt[c];
-        if (n_in > ORC_GRID_LEAF && depth + 1 < ORC_GRID_DEPTH && ext[c] / n_in < 2.0 * child_cell) {
+        if (n_in > ORC_GRID_LEAF && depth + 1 < ORC_GRID_DEPTH && ext[c] / n_in < 4.0 * child_cell) {
             int x = (int)(c % res), y = (int)((c / res) % res), z = (int)(c / ((long long)res * res));
             double clo[3] = {L.lo[0] + x * L.cell[0], L.lo[1] + y * L.cell[1], L.lo[2] + z * L.cell[2]};
             double chi[3] = {clo[0] + L.cell[0], clo[1] + L.cell[1], clo[2] + L.cell[2]};

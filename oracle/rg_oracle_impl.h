@@ -288,12 +288,16 @@ typedef struct {
 } ORC_FN(scene_);
 #define SCENE ORC_FN(scene_)
 
-/* Per-thread scratch of the candidate gathering. */
-typedef struct { unsigned char* mark; int* ids; long long* key; } ORC_FN(gscratch_);
-#define GSCRATCH ORC_FN(gscratch_)
-
 typedef struct { int g; REAL r1, r2; } ORC_FN(cand_);
 #define CAND ORC_FN(cand_)
+
+typedef struct { REAL r1; int k; } ORC_FN(r1key_);
+#define R1KEY ORC_FN(r1key_)
+
+/* Per-thread scratch of the candidate gathering and the slab sweep. */
+typedef struct { unsigned char* mark; int* ids; long long* key; R1KEY* by_r1; int* active; CAND* tmp; } ORC_FN(gscratch_);
+#define GSCRATCH ORC_FN(gscratch_)
+
 
 /* tea<4> seeding and LCG draws (forward/gaussians_aabb.h:63-94, a published TEA variant) */
 static unsigned ORC_FN(tea4)(unsigned v0, unsigned v1) {
@@ -416,8 +420,14 @@ static int ORC_FN(gather_cands)(const SCENE* S, const REAL* aabb, V3 o, V3 d, RE
         double span = 1e-6 * (fabs((double)tenter) + fabs((double)texit)) + 1e-9;
         int k = orc_grid_query(S->grid, oo, dd, (double)tenter - span, (double)texit + span, gs->mark, gs->ids);
         orc_grid_unmark(gs->mark, gs->ids, k);
-        orc_grid_sort(gs->ids, k, S->rank, gs->key);
+        /* test first, then sort the (few) passing candidates into candidate order */
         for (int j = 0; j < k; ++j) m += ORC_FN(cand_test)(S, aabb, gs->ids[j], o, d, invd, tenter, texit, out + m);
+        for (int j = 0; j < m; ++j) gs->ids[j] = j;
+        for (int j = 0; j < m; ++j)
+            gs->key[j] = ((long long)(S->rank ? S->rank[out[j].g] : out[j].g) << 32) | (unsigned)j;
+        qsort(gs->key, (size_t)m, sizeof(long long), orc_grid_cmp_ll);
+        for (int j = 0; j < m; ++j) gs->tmp[j] = out[(int)(gs->key[j] & 0xffffffffLL)];
+        memcpy(out, gs->tmp, sizeof(CAND) * (size_t)m);
         return m;
     }
     for (int li = 0; li < S->n; ++li) {
@@ -459,12 +469,18 @@ static void ORC_FN(gscratch_alloc)(GSCRATCH* gs, int n) {
     gs->mark = (unsigned char*)calloc(m, 1);
     gs->ids = (int*)malloc(sizeof(int) * m);
     gs->key = (long long*)malloc(sizeof(long long) * m);
+    gs->by_r1 = (R1KEY*)malloc(sizeof(R1KEY) * m);
+    gs->tmp = (CAND*)malloc(sizeof(CAND) * m);
+    gs->active = (int*)malloc(sizeof(int) * m);
 }
 
 static void ORC_FN(gscratch_free)(GSCRATCH* gs) {
     free(gs->mark);
     free(gs->ids);
     free(gs->key);
+    free(gs->by_r1);
+    free(gs->tmp);
+    free(gs->active);
 }
 
 #define ORC_BUF 8
@@ -521,10 +537,62 @@ static void ORC_FN(slab_buffers)(const SCENE* S, const int* hits, int nh, REAL t
 
 /* Per-slab hit list with the reference's cap semantics (forward/gaussians_aabb.cu:621-641):
  * at most max_prim_slice hits are kept; every further hit counts one overflow. */
-static int ORC_FN(slab_hits)(const CAND* cands, int nc, REAL lo, REAL hi, int cap, int* hits,
-                             long long* overflow) {
+/* The hits of one slab query [lo, hi] among a ray's candidates, in candidate order, at most `cap`
+ * (the any-hit cap, forward/gaussians_aabb.cu:621-641).  The queries of a ray move forward (lo and
+ * hi never decrease), so a sweep keeps an active list in candidate order: a candidate enters when
+ * r1 <= hi and leaves once r2 < lo, after which the exact test can no longer pass.  The active
+ * entries get the exact test, so the result is that of testing every candidate (the scan below,
+ * used when the prefilters are switched off). */
+typedef struct {
+    const CAND* cands; int nc;
+    R1KEY* by_r1; int next;          /* candidates by increasing r1 (ties: candidate order) */
+    int* active; int n_active;       /* candidate positions, increasing */
+    int sweep;
+} ORC_FN(sweep_);
+#define SWEEP ORC_FN(sweep_)
+
+static int ORC_FN(r1key_cmp)(const void* a, const void* b) {
+    const R1KEY* x = (const R1KEY*)a;
+    const R1KEY* y = (const R1KEY*)b;
+    if (x->r1 < y->r1) return -1;
+    if (x->r1 > y->r1) return 1;
+    return x->k - y->k;
+}
+
+static void ORC_FN(sweep_init)(SWEEP* sw, const CAND* cands, int nc, R1KEY* by_r1, int* active) {
+    sw->cands = cands; sw->nc = nc; sw->by_r1 = by_r1; sw->active = active;
+    sw->next = 0; sw->n_active = 0;
+    sw->sweep = orc_grid_enabled;
+    if (!sw->sweep) return;
+    for (int k = 0; k < nc; ++k) { by_r1[k].r1 = cands[k].r1; by_r1[k].k = k; }
+    qsort(by_r1, (size_t)nc, sizeof(R1KEY), ORC_FN(r1key_cmp));
+}
+
+static int ORC_FN(slab_hits)(SWEEP* sw, REAL lo, REAL hi, int cap, int* hits, long long* overflow) {
+    const CAND* cands = sw->cands;
     int nh = 0;
-    for (int k = 0; k < nc; ++k) {
+    if (!sw->sweep) {
+        for (int k = 0; k < sw->nc; ++k) {
+            if (!ORC_FN(slab_hit)(lo, hi, cands[k].r1, cands[k].r2)) continue;
+            if (nh >= cap) { ++*overflow; break; }
+            hits[nh++] = cands[k].g;
+        }
+        return nh;
+    }
+    while (sw->next < sw->nc && sw->by_r1[sw->next].r1 <= hi) {
+        int k = sw->by_r1[sw->next++].k, j = sw->n_active++;
+        while (j > 0 && sw->active[j - 1] > k) { sw->active[j] = sw->active[j - 1]; --j; }
+        sw->active[j] = k;
+    }
+    int keep = 0;
+    for (int j = 0; j < sw->n_active; ++j) {
+        int k = sw->active[j];
+        if (cands[k].r2 < lo) continue;     /* behind the ray's queries from here on */
+        sw->active[keep++] = k;
+    }
+    sw->n_active = keep;
+    for (int j = 0; j < sw->n_active; ++j) {
+        int k = sw->active[j];
         if (!ORC_FN(slab_hit)(lo, hi, cands[k].r1, cands[k].r2)) continue;
         if (nh >= cap) { ++*overflow; break; }
         hits[nh++] = cands[k].g;
@@ -562,13 +630,15 @@ int ORC_FN(orc_render_forward)(int n, const REAL* pos, const REAL* scl, const RE
             V3 col = MK(0, 0, 0);
             if (tenter < texit) {
                 int nc = ORC_FN(gather_cands)(&S, aabb, o, d, tenter, texit, order, cands, &gs);
+                SWEEP sw;
+                ORC_FN(sweep_init)(&sw, cands, nc, gs.by_r1, gs.active);
                 const REAL slab = ORC_DT * (REAL)ORC_BUF;
                 REAL tb = tenter;
                 while (tb < texit && T > ORC_TEPS) {
                     REAL lo = FMX(tenter, tb), hi = FMN(texit, tb + slab);
                     if (hi > tenter) {
                         ++st2;
-                        int nh = ORC_FN(slab_hits)(cands, nc, lo, hi, cap, hits, &st0);
+                        int nh = ORC_FN(slab_hits)(&sw, lo, hi, cap, hits, &st0);
                         if (nh > 0) {
                             st1 += nh;
                             REAL sig[ORC_BUF]; V3 C[ORC_BUF];
@@ -670,11 +740,13 @@ int ORC_FN(orc_render_inference)(int n, const REAL* pos, const REAL* scl, const 
                 const REAL slab = ORC_DT * (REAL)ORC_BUF;
                 /* candidates over the whole marched range: the last slab reaches past texit */
                 int nc = ORC_FN(gather_cands)(&S, aabb, o, d, tenter, texit + slab, order, cands, &gs);
+                SWEEP sw;
+                ORC_FN(sweep_init)(&sw, cands, nc, gs.by_r1, gs.active);
                 REAL tb = tenter;
                 while (tb < texit && T > ORC_TEPS) {
                     REAL lo = tb, hi = tb + slab;
                     if (hi > tenter) {
-                        int nh = ORC_FN(slab_hits)(cands, nc, lo, hi, cap, hits, &st0);
+                        int nh = ORC_FN(slab_hits)(&sw, lo, hi, cap, hits, &st0);
                         if (nh > 0) {
                             st1 += nh;
                             cnt += nh < ccap ? nh : ccap;
@@ -737,6 +809,8 @@ int ORC_FN(orc_render_backward)(int n, const REAL* pos, const REAL* scl, const R
             ORC_FN(scene_clip)(scene_box, o, d, &tenter, &texit);
             if (!(tenter < texit)) continue;
             int nc = ORC_FN(gather_cands)(&S, aabb, o, d, tenter, texit, order, cands, &gs);
+            SWEEP sw;
+            ORC_FN(sweep_init)(&sw, cands, nc, gs.by_r1, gs.active);
             const REAL slab = ORC_DT * (REAL)ORC_BUF;
             REAL tb = tenter;
             REAL Tb = 1;
@@ -745,7 +819,7 @@ int ORC_FN(orc_render_backward)(int n, const REAL* pos, const REAL* scl, const R
             while (tb < texit && Tb > ORC_TEPS) {
                 REAL lo = FMX(tenter, tb), hi = FMN(texit, tb + slab);
                 if (hi > tenter) {
-                    int nh = ORC_FN(slab_hits)(cands, nc, lo, hi, cap, hits, &st0);
+                    int nh = ORC_FN(slab_hits)(&sw, lo, hi, cap, hits, &st0);
                     if (nh == 0) { tb += slab; continue; }
                     st1 += nh;
                     REAL sig[ORC_BUF]; V3 C[ORC_BUF];
@@ -866,6 +940,8 @@ int ORC_FN(orc_render_backward)(int n, const REAL* pos, const REAL* scl, const R
 #undef CAND
 #undef GSCRATCH
 #undef GRIDSET
+#undef SWEEP
+#undef R1KEY
 #undef GAUSS
 #undef ORC_BUF
 #undef ORC_DT
