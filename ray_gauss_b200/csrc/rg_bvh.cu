@@ -4,6 +4,7 @@
 // Reference: the AABB formula is optix_raycasting/optix_utils.py:34-66 and the scene box
 // render_optix.py:105-106; the BVH replaces the OptiX GAS built by optix_utils.py:68-75.
 #include <cub/device/device_radix_sort.cuh>
+#include <cub/device/device_scan.cuh>
 
 #include <climits>
 
@@ -260,39 +261,74 @@ __global__ void k_refit(int n, const float4* __restrict__ leaf_lo, const float4*
     }
 }
 
-// 4-wide traversal nodes.  Every internal node i at even depth gets the four grandchildren under
-// its two children as two halves in the binary node format (half 0 under the left child, half 1
-// under the right one): an internal child contributes its own node (both child boxes, ids and
-// leaf ranges), a leaf child contributes itself in slot 0 of its half and an empty slot 1 whose
-// range end (INT_MIN) never passes the traversal's cursor test.  Children stay in leaf order.
-// Internal grandchildren are at even depth again, so the 4-wide tree is indexed by binary index.
-__global__ void k_collapse(int n, const Node* __restrict__ nodes, const int* __restrict__ node_parent,
-                           Node* __restrict__ nodes4) {
+// Depth of every binary node below the root (walk to the root; a few dozen steps).
+__global__ void k_depth(int n, const int* __restrict__ node_parent, int* __restrict__ depth) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n - 1) return;
-    int odd = 0;
-    int p = i;
-    for (int k = 0; k < 4096; ++k) {
-        p = node_parent[p];
-        if (p < 0) break;
-        odd ^= 1;
-    }
-    if (odd) return;
-    const Node nd = nodes[i];
-    const float* f = reinterpret_cast<const float*>(&nd);
-    for (int h = 0; h < 2; ++h) {
-        const int c = h == 0 ? nd.n3.x : nd.n3.y;
-        Node half;
-        if (c >= 0) {
-            half = nodes[c];
+    int d = 0;
+    for (int p = node_parent[i]; p >= 0 && d < 4096; p = node_parent[p]) ++d;
+    depth[i] = d;
+}
+
+// Frontier of the wide node at binary node i, in leaf order (depth-first, left child first): every
+// binary descendant kWideLevels levels down and every leaf reached before.  Calls emit(k, id, box)
+// for the k-th child; the box of a child is the one its binary parent stores for it.
+template <typename Emit>
+__device__ __forceinline__ int wide_frontier(const Node* __restrict__ nodes, int i, Emit emit) {
+    struct Entry { int id, level; float b[6]; };
+    Entry st[kWideLevels + 2];
+    int sp = 0, k = 0;
+    auto push_children = [&](int p, int level) {
+        const Node nd = nodes[p];
+        const float* f = reinterpret_cast<const float*>(&nd);
+        Entry r{nd.n3.y, level, {f[6], f[7], f[8], f[9], f[10], f[11]}};
+        Entry l{nd.n3.x, level, {f[0], f[1], f[2], f[3], f[4], f[5]}};
+        st[sp++] = r;
+        st[sp++] = l;
+    };
+    push_children(i, 1);
+    while (sp > 0) {
+        const Entry e = st[--sp];
+        if (e.id < 0 || e.level == kWideLevels) {
+            emit(k, e.id, e.b);
+            ++k;
         } else {
-            float* hf = reinterpret_cast<float*>(&half);
-            for (int k = 0; k < 6; ++k) hf[k] = f[6 * h + k];
-            for (int k = 6; k < 12; ++k) hf[k] = 0.f;
-            half.n3 = make_int4(c, c, h == 0 ? nd.n3.z : nd.n3.w, INT_MIN);
+            push_children(e.id, e.level + 1);
         }
-        nodes4[2 * (long long)i + h] = half;
     }
+    return k;
+}
+
+// Children of every wide node (binary nodes at depths that are multiples of kWideLevels).
+__global__ void k_wide_count(int n, const Node* __restrict__ nodes, const int* __restrict__ depth,
+                             int* __restrict__ cnt) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n - 1) return;
+    cnt[i] = (depth[i] % kWideLevels == 0) ? wide_frontier(nodes, i, [](int, int, const float*) {}) : 0;
+}
+
+__global__ void k_wide_table(int n, const int* __restrict__ cnt, const int* __restrict__ begin,
+                             int2* __restrict__ tab) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n - 1) return;
+    tab[i] = make_int2(begin[i], cnt[i]);
+}
+
+// Slots of every wide node from the refitted binary boxes (after every build and refit).
+__global__ void k_wide_fill(int n, const Node* __restrict__ nodes, const int2* __restrict__ tab,
+                            WideSlot* __restrict__ slots) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n - 1) return;
+    const int2 t = tab[i];
+    if (t.y == 0) return;
+    WideSlot* out = slots + t.x;
+    wide_frontier(nodes, i, [&](int k, int id, const float* b) {
+        WideSlot sl;
+        for (int a = 0; a < 3; ++a) { sl.lo[a] = b[a]; sl.hi[a] = b[3 + a]; }
+        sl.id = id;
+        sl.range_hi = id < 0 ? ~id : nodes[id].n3.w;
+        out[k] = sl;
+    });
 }
 
 // ---- host launchers --------------------------------------------------------------------------
@@ -313,12 +349,14 @@ cudaError_t launch_scene_out(const int* scene_ord, float* out, cudaStream_t s) {
     return cudaGetLastError();
 }
 
+// Temporary storage of the radix sort and of the wide-node slot scan (they run one after the other).
 size_t sort_temp_bytes(long long n) {
-    size_t bytes = 0;
+    size_t bytes = 0, scan = 0;
     cub::DeviceRadixSort::SortPairs(nullptr, bytes, (const unsigned long long*)nullptr,
                                     (unsigned long long*)nullptr, (const int*)nullptr, (int*)nullptr, (int)n, 0,
                                     63);
-    return bytes;
+    cub::DeviceScan::ExclusiveSum(nullptr, scan, (const int*)nullptr, (int*)nullptr, (int)(n > 1 ? n - 1 : 1));
+    return bytes > scan ? bytes : scan;
 }
 
 cudaError_t launch_refit_only(long long n, BvhBuffers& b, cudaStream_t s);
@@ -336,18 +374,30 @@ cudaError_t launch_build(long long n, const float* aabb, const int* scene_ord, c
     if (n > 1) {
         int ib = (int)((n - 1 + 255) / 256);
         k_karras<<<ib, 256, 0, s>>>((int)n, b.keys_out, b.nodes, b.leaf_parent, b.node_parent);
+        // wide-node layout (topology only): depths, children per wide node, first slots
+        k_depth<<<ib, 256, 0, s>>>((int)n, b.node_parent, b.depth);
+        k_wide_count<<<ib, 256, 0, s>>>((int)n, b.nodes, b.depth, b.wide_cnt);
+        size_t sbytes = b.sort_temp_bytes;
+        err = cub::DeviceScan::ExclusiveSum(b.sort_temp, sbytes, b.wide_cnt, b.depth, (int)(n - 1), s);
+        if (err != cudaSuccess) return err;
+        // the scan overwrote the depths with the first slots; the table keeps {first slot, count}
+        k_wide_table<<<ib, 256, 0, s>>>((int)n, b.wide_cnt, b.depth, b.wide_tab);
     }
     return launch_refit_only(n, b, s);
 }
 
 cudaError_t launch_refit_only(long long n, BvhBuffers& b, cudaStream_t s) {
-    if (n > 1) cudaMemsetAsync(b.refit_cnt, 0, sizeof(unsigned) * (size_t)(n - 1), s);
+    if (n > 1) {
+        // the refit counters must start at zero (the allocation-free path's array keeps old contents)
+        const cudaError_t err = cudaMemsetAsync(b.refit_cnt, 0, sizeof(unsigned) * (size_t)(n - 1), s);
+        if (err != cudaSuccess) return err;
+    }
     int blocks = (int)((n + 255) / 256);
     k_refit<<<blocks, 256, 0, s>>>((int)n, b.leaf_lo, b.leaf_hi, b.nodes, b.leaf_parent, b.node_parent, b.refit_cnt,
                                    b.root_box);
     if (n > 1) {
         int ib = (int)((n - 1 + 255) / 256);
-        k_collapse<<<ib, 256, 0, s>>>((int)n, b.nodes, b.node_parent, b.nodes4);
+        k_wide_fill<<<ib, 256, 0, s>>>((int)n, b.nodes, b.wide_tab, b.slots);
     }
     return cudaGetLastError();
 }

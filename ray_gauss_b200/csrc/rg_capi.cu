@@ -84,7 +84,10 @@ int ensure_n(rg_engine* e, long long n) {
     if ((rc = grow(e, e->bvh.leaf_lo, N))) return rc;
     if ((rc = grow(e, e->bvh.leaf_hi, N))) return rc;
     if ((rc = grow(e, e->bvh.nodes, N > 1 ? N - 1 : 1))) return rc;
-    if ((rc = grow(e, e->bvh.nodes4, N > 1 ? 2 * (N - 1) : 2))) return rc;
+    if ((rc = grow(e, e->bvh.depth, N > 1 ? N - 1 : 1))) return rc;
+    if ((rc = grow(e, e->bvh.wide_cnt, N > 1 ? N - 1 : 1))) return rc;
+    if ((rc = grow(e, e->bvh.wide_tab, N > 1 ? N - 1 : 1))) return rc;
+    if ((rc = grow(e, e->bvh.slots, 2 * N))) return rc;
     if ((rc = grow(e, e->bvh.leaf_parent, N))) return rc;
     if ((rc = grow(e, e->bvh.node_parent, N > 1 ? N - 1 : 1))) return rc;
     if ((rc = grow(e, e->bvh.refit_cnt, N > 1 ? N - 1 : 1))) return rc;
@@ -163,12 +166,24 @@ int check_table(long long n, int n_cams) {
 
 cudaStream_t S(void* s) { return reinterpret_cast<cudaStream_t>(s); }
 
-int set_device(rg_engine* e) {
-    int cur = -1;
-    cudaGetDevice(&cur);
-    if (cur != e->device) RG_CUDA(cudaSetDevice(e->device), "cudaSetDevice");
-    return RG_OK;
-}
+// Makes the engine's device current for one entry point and restores the caller's current device
+// when the entry point returns, so a call on an engine of another device leaves the caller's (and
+// torch's) notion of the current device unchanged.
+struct DeviceScope {
+    int prev = -1;
+    bool switched = false;
+    int enter(rg_engine* e) {
+        if (cudaGetDevice(&prev) != cudaSuccess) prev = -1;
+        if (prev != e->device) {
+            RG_CUDA(cudaSetDevice(e->device), "cudaSetDevice");
+            switched = prev >= 0;
+        }
+        return RG_OK;
+    }
+    ~DeviceScope() {
+        if (switched) cudaSetDevice(prev);
+    }
+};
 
 // The fast kernels run only without random sample offsets (launch_render picks the same way).
 int kernel_mode(const rg_settings* s) {
@@ -190,7 +205,8 @@ int fill_args(rg_engine* e, const rg_camera* cams, const rg_settings* s, rg::Ren
     a.is_rec = e->bvh.leaf_is;
     a.ext = e->bvh.leaf_ext;
     a.rgb = e->rgb_leaf;
-    a.nodes4 = e->bvh.nodes4;
+    a.wide_tab = e->bvh.wide_tab;
+    a.slots = e->bvh.slots;
     a.n_leaves = (int)e->n_built;
     a.scene_ord = e->scene_ord;
     a.white_bg = s->white_background;
@@ -206,6 +222,26 @@ int fill_args(rg_engine* e, const rg_camera* cams, const rg_settings* s, rg::Ren
 }
 
 }  // namespace
+
+void rg::export_status(const DevStatus& h, rg_status* out) {
+    out->hit_pairs = h.hit_pairs;
+    out->slabs = h.slabs;
+    out->slab_cap_exceeded = h.slab_cap_exceeded;
+    out->list_passes = h.list_passes;
+    out->chunk_splits = h.chunk_splits;
+    out->stack_overflows = h.stack_overflows;
+    out->watchdog_trips = h.watchdog_trips;
+    out->nonfinite_inputs = h.nonfinite_inputs;
+    out->traversals = h.traversals;
+    out->node_visits = h.node_visits;
+    out->leaf_tests = h.leaf_tests;
+    out->list_entries = h.list_entries;
+    out->slab_steps = h.slab_steps;
+    out->entry_slabs = h.entry_slabs;
+    out->replayed_chunks = h.replayed_chunks;
+    out->record_overflows = h.record_overflows;
+    out->record_words = 0;
+}
 
 extern "C" {
 
@@ -234,7 +270,8 @@ int rg_create(rg_engine** out, int device) {
     rg_engine* e = new (std::nothrow) rg_engine();
     if (!e) return RG_ERR_OOM;
     e->device = device;
-    int rc = set_device(e);
+    DeviceScope dev_scope;
+    int rc = dev_scope.enter(e);
     if (rc) { delete e; return rc; }
     cudaDeviceGetAttribute(&e->num_sms, cudaDevAttrMultiProcessorCount, device);
     if ((rc = grow(e, e->scene_ord, 6)) || (rc = grow(e, e->vt, 1)) || (rc = grow(e, e->work_counter, 4)) ||
@@ -249,10 +286,11 @@ int rg_create(rg_engine** out, int device) {
 
 int rg_destroy(rg_engine* e) {
     if (!e) return RG_OK;
-    set_device(e);
+    DeviceScope dev_scope;
+    dev_scope.enter(e);
     void* ptrs[] = {e->rec, e->aabb, e->scene_ord, e->bvh.keys_in, e->bvh.keys_out, e->bvh.vals_in, e->bvh.leaf_gid,
                     e->bvh.rank, e->bvh.leaf_rec, e->bvh.leaf_is, e->bvh.leaf_ext, e->bvh.leaf_lo, e->bvh.leaf_hi, e->bvh.nodes,
-                    e->bvh.nodes4,
+                    e->bvh.depth, e->bvh.wide_cnt, e->bvh.wide_tab, e->bvh.slots,
                     e->bvh.leaf_parent, e->bvh.node_parent, e->bvh.refit_cnt, e->bvh.root_box, e->bvh.sort_temp,
                     e->rgb_leaf, e->gacc_geo, e->gacc_rgb, e->vt, e->work_counter, e->st, e->rec_arena,
                     e->rec_top, e->rec_tile};
@@ -264,7 +302,8 @@ int rg_destroy(rg_engine* e) {
 
 int rg_reserve(rg_engine* e, int64_t n, int32_t n_views, int64_t n_rays) {
     if (!e || n < 0 || n_views < 0 || n_views > rg::kMaxViews) return RG_ERR_INVALID_ARG;
-    int rc = set_device(e);
+    DeviceScope dev_scope;
+    int rc = dev_scope.enter(e);
     if (rc) return rc;
     if (n > 0 && (rc = ensure_n(e, n))) return rc;
     if (n_views > 0 && (rc = ensure_views(e, n_views))) return rc;
@@ -302,7 +341,8 @@ int rg_ellipsoids_bbox(rg_engine* e, const rg_gaussians* g, float* aabb_out, flo
     if (!e) return RG_ERR_INVALID_ARG;
     int rc = check_gaussians(g);
     if (rc) return rc;
-    if ((rc = set_device(e))) return rc;
+    DeviceScope dev_scope;
+    if ((rc = dev_scope.enter(e))) return rc;
     if ((rc = ensure_n(e, g->n))) return rc;
     RG_CUDA(rg::launch_prepass(g, e->rec, e->aabb, e->scene_ord, e->st, S(stream)), "prepass");
     e->launches += 2;
@@ -325,7 +365,8 @@ int rg_ellipsoids_bbox(rg_engine* e, const rg_gaussians* g, float* aabb_out, flo
 int rg_bvh_build(rg_engine* e, void* stream) {
     if (!e || e->n_bbox <= 0) return RG_ERR_STATE;
     const rg_gaussians* g = &e->g_bbox;
-    int rc = set_device(e);
+    DeviceScope dev_scope;
+    int rc = dev_scope.enter(e);
     if (rc) return rc;
     RG_CUDA(rg::launch_build(e->n_bbox, e->aabb, e->scene_ord, e->rec, g, e->bvh, S(stream)), "bvh build");
     e->launches += 6;
@@ -338,7 +379,8 @@ int rg_bvh_build(rg_engine* e, void* stream) {
 int rg_bvh_refit(rg_engine* e, void* stream) {
     if (!e || e->n_bbox <= 0 || e->n_built != e->n_bbox) return RG_ERR_STATE;
     const rg_gaussians* g = &e->g_bbox;
-    int rc = set_device(e);
+    DeviceScope dev_scope;
+    int rc = dev_scope.enter(e);
     if (rc) return rc;
     RG_CUDA(rg::launch_refit(e->n_built, e->aabb, e->rec, g, e->bvh, S(stream)), "bvh refit");
     e->launches += 2;
@@ -355,7 +397,8 @@ int rg_forward_sh(rg_engine* e, const rg_gaussians* g, const rg_camera* cams, in
     if (rc || (rc = check_views(cams, n_cams))) return rc;
     if (e->n_built != g->n) return RG_ERR_STATE;
     if ((rc = check_table(g->n, n_cams))) return rc;
-    if ((rc = set_device(e)) || (rc = ensure_views(e, n_cams))) return rc;
+    DeviceScope dev_scope;
+    if ((rc = dev_scope.enter(e)) || (rc = ensure_views(e, n_cams))) return rc;
     RG_CUDA(rg::launch_color_forward(g, cams, n_cams, e->bvh.rank, e->rgb_leaf, rgb_out, S(stream)), "forward_sh");
     e->launches += 1;
     e->colors_views = n_cams;
@@ -369,7 +412,8 @@ int rg_launch_forward(rg_engine* e, const rg_camera* cams, int32_t n_cams, const
     int rc = check_views(cams, n_cams);
     if (rc) return rc;
     if (e->n_built <= 0 || e->colors_views < n_cams) return RG_ERR_STATE;
-    if ((rc = set_device(e))) return rc;
+    DeviceScope dev_scope;
+    if ((rc = dev_scope.enter(e))) return rc;
     RG_CUDA(rg::launch_setup_views(cams, n_cams, e->vt, e->work_counter, S(stream)), "setup views");
     rg::RenderArgs a;
     fill_args(e, cams, s, a);
@@ -403,7 +447,8 @@ int rg_launch_inference(rg_engine* e, const rg_camera* cams, int32_t n_cams, con
     int rc = check_views(cams, n_cams);
     if (rc) return rc;
     if (e->n_built <= 0 || e->colors_views < n_cams) return RG_ERR_STATE;
-    if ((rc = set_device(e))) return rc;
+    DeviceScope dev_scope;
+    if ((rc = dev_scope.enter(e))) return rc;
     // the inference programs sample without jitter or random offsets
     rg_settings si = *s;
     si.jitter = 0;
@@ -438,7 +483,8 @@ int rg_launch_backward(rg_engine* e, const rg_camera* cams, int32_t n_cams, cons
     int rc = check_views(cams, n_cams);
     if (rc) return rc;
     if (e->n_built <= 0 || e->colors_views < n_cams) return RG_ERR_STATE;
-    if ((rc = set_device(e))) return rc;
+    DeviceScope dev_scope;
+    if ((rc = dev_scope.enter(e))) return rc;
     size_t N = (size_t)e->n_built;
     RG_CUDA(cudaMemsetAsync(e->gacc_geo, 0, sizeof(float4) * 3 * N, S(stream)), "zero grads");
     RG_CUDA(cudaMemsetAsync(e->gacc_rgb, 0, sizeof(float4) * N * (size_t)n_cams, S(stream)), "zero grads");
@@ -477,7 +523,8 @@ int rg_backward_sh(rg_engine* e, const rg_gaussians* g, const rg_camera* cams, i
     if (g->num_sph_gauss > 0 && (!out->sph_gauss_features || !out->bandwidth_sharpness || !out->lobe_axis))
         return RG_ERR_INVALID_ARG;
     if (e->n_built != g->n) return RG_ERR_STATE;
-    if ((rc = set_device(e))) return rc;
+    DeviceScope dev_scope;
+    if ((rc = dev_scope.enter(e))) return rc;
     RG_CUDA(rg::launch_color_backward(g, cams, n_cams, e->bvh.rank, e->gacc_geo, e->gacc_rgb, s->sh_quirk, out,
                                       S(stream)),
             "backward_sh");
@@ -508,7 +555,8 @@ int rg_render_backward(rg_engine* e, const rg_gaussians* g, const rg_camera* cam
 int rg_leaf_order(rg_engine* e, int32_t* leaf_gid_out, void* stream) {
     if (!e || !leaf_gid_out) return RG_ERR_INVALID_ARG;
     if (e->n_built <= 0) return RG_ERR_STATE;
-    int rc = set_device(e);
+    DeviceScope dev_scope;
+    int rc = dev_scope.enter(e);
     if (rc) return rc;
     RG_CUDA(cudaMemcpyAsync(leaf_gid_out, e->bvh.leaf_gid, sizeof(int32_t) * (size_t)e->n_built,
                             cudaMemcpyDeviceToDevice, S(stream)),
@@ -518,28 +566,13 @@ int rg_leaf_order(rg_engine* e, int32_t* leaf_gid_out, void* stream) {
 
 int rg_get_status(rg_engine* e, rg_status* out, int32_t reset, void* stream) {
     if (!e || !out) return RG_ERR_INVALID_ARG;
-    int rc = set_device(e);
+    DeviceScope dev_scope;
+    int rc = dev_scope.enter(e);
     if (rc) return rc;
     RG_CUDA(cudaStreamSynchronize(S(stream)), "sync");
     rg::DevStatus h;
     RG_CUDA(cudaMemcpy(&h, e->st, sizeof(h), cudaMemcpyDeviceToHost), "read status");
-    out->hit_pairs = h.hit_pairs;
-    out->slabs = h.slabs;
-    out->slab_cap_exceeded = h.slab_cap_exceeded;
-    out->list_passes = h.list_passes;
-    out->chunk_splits = h.chunk_splits;
-    out->stack_overflows = h.stack_overflows;
-    out->watchdog_trips = h.watchdog_trips;
-    out->nonfinite_inputs = h.nonfinite_inputs;
-    out->traversals = h.traversals;
-    out->node_visits = h.node_visits;
-    out->leaf_tests = h.leaf_tests;
-    out->list_entries = h.list_entries;
-    out->slab_steps = h.slab_steps;
-    out->entry_slabs = h.entry_slabs;
-    out->replayed_chunks = h.replayed_chunks;
-    out->record_overflows = h.record_overflows;
-    out->record_words = 0;
+    rg::export_status(h, out);
     if (e->rec_top) {
         unsigned long long w = 0;
         RG_CUDA(cudaMemcpy(&w, e->rec_top, sizeof(w), cudaMemcpyDeviceToHost), "read record size");

@@ -20,7 +20,7 @@ constexpr int kWarp = 32;
 constexpr int kTileW = 8;               // a warp renders an 8x4 pixel tile
 constexpr int kTileH = 4;
 constexpr int kMaxChunk = 255;          // slabs per traversal chunk (slab ranges are bytes)
-constexpr int kStack = 96;              // warp traversal stack depth
+constexpr int kStack = 192;             // warp traversal stack depth (up to 31 pushes per wide node)
 
 // Device status block (mirrors rg_status) + work counters.
 struct DevStatus {
@@ -139,6 +139,19 @@ struct __align__(16) LeafIS {
 struct __align__(16) GaussRec {
     LeafRec s;
     LeafIS is;
+};
+
+// Wide traversal nodes.  Every binary node at a depth that is a multiple of kWideLevels owns the
+// frontier of its subtree kWideLevels levels down (binary nodes there, or leaves reached earlier):
+// at most kWideSlots children, stored as consecutive slots in leaf order.  A slot holds the child's
+// box, its id (>= 0 the binary index of a wide node, < 0 leaf ~index) and the last leaf of its
+// subtree (the multi-pass cursor test).  32 bytes, read with one 256-bit load per lane.
+constexpr int kWideLevels = 5;
+constexpr int kWideSlots = 1 << kWideLevels;
+struct __align__(32) WideSlot {
+    float lo[3], hi[3];
+    int id;
+    int range_hi;
 };
 
 // BVH internal node, 64 bytes: child boxes, child ids (>= 0 internal, < 0 leaf ~id),

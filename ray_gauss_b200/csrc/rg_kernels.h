@@ -17,7 +17,10 @@ struct BvhBuffers {
     float4* leaf_lo = nullptr;
     float4* leaf_hi = nullptr;
     Node* nodes = nullptr;
-    Node* nodes4 = nullptr;       // 4-wide traversal nodes: two binary-format halves per binary node
+    int* depth = nullptr;         // per binary node: depth below the root
+    int* wide_cnt = nullptr;      // per binary node: wide children (0 unless a wide node)
+    int2* wide_tab = nullptr;     // per binary node: {first slot, slot count} of its wide node
+    WideSlot* slots = nullptr;    // wide-node children (at most 2n slots)
     int* leaf_parent = nullptr;
     int* node_parent = nullptr;
     unsigned* refit_cnt = nullptr;
@@ -33,7 +36,8 @@ struct RenderArgs {
     const LeafIS* is_rec;
     const float4* ext;
     const float4* rgb;            // (n_views, n_leaves) leaf order
-    const Node* nodes4;           // 4-wide traversal nodes (halves 2i, 2i+1 of internal node i)
+    const int2* wide_tab;         // wide node of binary node i: {first slot, slot count}
+    const WideSlot* slots;        // wide-node children
     int n_leaves;
     const int* scene_ord;
     int white_bg, jitter, rnd_sample, max_prim_slice;
@@ -88,5 +92,9 @@ cudaError_t launch_render(bool backward, int mode, int cap, int grid, const Rend
 int render_block_threads();
 int render_occupancy(bool backward, int mode, int cap);
 size_t render_smem_bytes(bool backward, int cap);
+
+// Copies a device status block read back to the host into the public struct (record_words is left
+// to the caller).
+void export_status(const DevStatus& h, rg_status* out);
 
 }  // namespace rg

@@ -12,10 +12,11 @@
 //
 // Design.  A warp owns an 8x4 pixel tile (tiles of all views are pulled from one atomic work
 // counter).  Each lane marches its own ray with the reference's slab sequence (tb += 0.02 in
-// FP32); the warp advances in chunks of K slabs per lane (K adapts between 1 and 64: it grows
+// FP32); the warp advances in chunks of K slabs per lane (K adapts between 1 and 255: it grows
 // while hits are sparse and halves when the hit list overflows).  For a chunk the warp traverses
-// the LBVH once for the union of its lanes' segments with a warp-uniform stack, runs the exact
-// ellipsoid test per lane at the leaves and appends every leaf that any lane hits to a shared hit
+// the wide BVH once for the beam of its lanes' segments (one child slot per lane against the
+// beam's planes) with a warp-uniform stack, runs the exact ellipsoid test per lane at the leaves
+// and appends every leaf that any lane hits to a shared hit
 // list with, per lane, the range of the chunk's slabs its interval covers (exact for K <= 8; one
 // slab of margin on each side for longer chunks, where the extra slabs' samples fall outside the
 // threshold ellipsoid and are masked out).  The list is consumed slab by slab: each lane evaluates
@@ -33,6 +34,8 @@
 // arithmetic.  RG_MODE_FAST evaluates the 8 samples of a slab from the quadratic form of the
 // Mahalanobis distance along the ray with the SFU exponential and accumulates the adjoint in
 // moment form.
+#include <cstddef>
+
 #include "rg_common.cuh"
 #include "rg_kernels.h"
 
@@ -52,6 +55,8 @@ constexpr int kCounters = 9;
 constexpr unsigned kNoRecord = 0xffffffffu;     // hit-list record: no (next) chunk record
 constexpr unsigned kRecordMulti = 0x80000000u;  // chunk consumed in several traversal passes
 constexpr unsigned kRecordFailed = 0xfffffffeu; // the tile's record did not fit the arena
+constexpr int kFrustumPlanes = 6;               // 4 sides through the eye, near and far along the axis
+constexpr int kFrustumFloats = 8 * kFrustumPlanes;
 
 // Warp hit-list layout.  Parity arithmetic keeps, per entry and lane, the exact range of the
 // chunk's slabs the lane's interval covers (64 B per entry); the fast arithmetic keeps only the mask
@@ -70,6 +75,7 @@ struct WarpSmem {
     unsigned short lrng[FAST ? 1 : CAP][32];         // parity: per lane lo | hi << 8 (lo > hi: no hit)
     unsigned smask[NB][CAP / 32];                    // entries whose union range meets block k / MB
     unsigned long long occ[4];                       // slabs holding any entry (union occupancy)
+    __align__(16) float frustum[kFrustumFloats];     // the chunk's beam: cull planes, read as float4
     int stack[kStack];
     // hit-list record of the warp's current tile (written by lane 0)
     unsigned rec_first, rec_prev;                    // forward: first / last chunk record
@@ -85,8 +91,7 @@ struct WarpStats {
 };
 
 struct RayState {
-    float3 o, d, invd;
-    float3 oid;   // -o * invd (fast box test)
+    float3 o, d;
     float tenter, texit;
     float tb;
     float T;
@@ -105,41 +110,104 @@ __device__ __forceinline__ float3 rows_rn(float3 r0, float3 r1, float3 r2, float
     return f3(dot_rn(r0, v), dot_rn(r1, v), dot_rn(r2, v));
 }
 
-// Slab test of a BVH box against [lo, hi].  The fast arithmetic evaluates t = b/d - o/d with one
-// FMA per plane; its rounding (~1e-7 of |o/d|) stays inside the leaf boxes' 1e-5 inflation for
-// scenes within a few hundred units of the camera.
-template <bool FAST>
-__device__ __forceinline__ bool box_hit(const float* bx, const RayState& r, float lo, float hi) {
-    float tx0, tx1, ty0, ty1, tz0, tz1;
-    if (FAST) {
-        tx0 = fmaf(bx[0], r.invd.x, r.oid.x); tx1 = fmaf(bx[3], r.invd.x, r.oid.x);
-        ty0 = fmaf(bx[1], r.invd.y, r.oid.y); ty1 = fmaf(bx[4], r.invd.y, r.oid.y);
-        tz0 = fmaf(bx[2], r.invd.z, r.oid.z); tz1 = fmaf(bx[5], r.invd.z, r.oid.z);
-    } else {
-        tx0 = (bx[0] - r.o.x) * r.invd.x; tx1 = (bx[3] - r.o.x) * r.invd.x;
-        ty0 = (bx[1] - r.o.y) * r.invd.y; ty1 = (bx[4] - r.o.y) * r.invd.y;
-        tz0 = (bx[2] - r.o.z) * r.invd.z; tz1 = (bx[5] - r.o.z) * r.invd.z;
-    }
-    float tn = fmaxf(max3f(fminf(tx0, tx1), fminf(ty0, ty1), fminf(tz0, tz1)), lo);
-    float tf = fminf(min3f(fmaxf(tx0, tx1), fmaxf(ty0, ty1), fmaxf(tz0, tz1)), hi);
-    return tn <= tf;
+// One wide-node child slot (32 bytes) in one 256-bit read-only load.
+__device__ __forceinline__ void load_slot(const WideSlot* p, float3& lo, float3& hi, int& id, int& range_hi) {
+    float f[6];
+    int u[2];
+    asm("ld.global.nc.v8.b32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
+        : "=f"(f[0]), "=f"(f[1]), "=f"(f[2]), "=f"(f[3]), "=f"(f[4]), "=f"(f[5]), "=r"(u[0]), "=r"(u[1])
+        : "l"(p));
+    lo = f3(f[0], f[1], f[2]);
+    hi = f3(f[3], f[4], f[5]);
+    id = u[0];
+    range_hi = u[1];
 }
 
-// A 64-byte node in two 256-bit read-only loads (nodes are 64-byte aligned).
-__device__ __forceinline__ void load_node(const Node* p, float (&lb)[6], float (&rb)[6], int4& n3) {
-    float f[8];
-    unsigned u[8];
-    asm("ld.global.nc.v8.f32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
-        : "=f"(f[0]), "=f"(f[1]), "=f"(f[2]), "=f"(f[3]), "=f"(f[4]), "=f"(f[5]), "=f"(f[6]), "=f"(f[7])
-        : "l"(p));
-    asm("ld.global.nc.v8.b32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
-        : "=r"(u[0]), "=r"(u[1]), "=r"(u[2]), "=r"(u[3]), "=r"(u[4]), "=r"(u[5]), "=r"(u[6]), "=r"(u[7])
-        : "l"(reinterpret_cast<const char*>(p) + 32));
-    lb[0] = f[0]; lb[1] = f[1]; lb[2] = f[2]; lb[3] = f[3]; lb[4] = f[4]; lb[5] = f[5];
-    rb[0] = f[6]; rb[1] = f[7];
-    rb[2] = __uint_as_float(u[0]); rb[3] = __uint_as_float(u[1]); rb[4] = __uint_as_float(u[2]);
-    rb[5] = __uint_as_float(u[3]);
-    n3 = make_int4((int)u[4], (int)u[5], (int)u[6], (int)u[7]);
+// Beam of a warp's chunk: the rays through the sample positions of the active lanes' pixel
+// rectangle (pixel centres; with jitter the [x + 1/3, x + 2/3) range the jittered samples take)
+// between the nearest start and the farthest end of the active lanes' chunk segments, measured
+// along the tile's central axis.  Six planes, each stored as the positive and
+// negative parts of its normal and an offset: a box lies outside when the largest value of n . x
+// over the box is below the offset.  The planes are widened by a slack far above the rounding of
+// the plane and box arithmetic, so the beam contains every ray segment the lanes test: the exact
+// per-lane leaf test decides the hits, the beam only skips subtrees no active ray can reach.
+__device__ __forceinline__ void set_plane(float* F, int i, float3 n, float off) {
+    F[8 * i + 0] = fmaxf(n.x, 0.f);
+    F[8 * i + 1] = fmaxf(n.y, 0.f);
+    F[8 * i + 2] = fmaxf(n.z, 0.f);
+    F[8 * i + 3] = fminf(n.x, 0.f);
+    F[8 * i + 4] = fminf(n.y, 0.f);
+    F[8 * i + 5] = fminf(n.z, 0.f);
+    F[8 * i + 6] = off;
+    F[8 * i + 7] = 0.f;
+}
+__device__ __forceinline__ float3 cross3(float3 a, float3 b) {
+    return f3(a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x);
+}
+// Unnormalised direction of the camera ray through image coordinates (u, v) in [0, 1]^2 (the ray
+// generation's d before normalisation, linear in u and v).
+__device__ __forceinline__ float3 pixel_dir(const rg_camera& cam, float u, float v) {
+    const float dx = (2.f * u - 1.f) * cam.tan_half_fovx, dy = (2.f * v - 1.f) * cam.tan_half_fovy;
+    return f3(cam.u[0] * dx + cam.v[0] * dy + cam.w[0], cam.u[1] * dx + cam.v[1] * dy + cam.w[1],
+              cam.u[2] * dx + cam.v[2] * dy + cam.w[2]);
+}
+
+template <bool FAST, int CAP>
+__device__ __forceinline__ void set_frustum(WarpSmem<FAST, CAP>& sm, const rg_camera& cam, int jitter, int px,
+                                            int py, const RayState& r, bool on, float seg_hi, int lane) {
+    const unsigned x0 = __reduce_min_sync(kFull, on ? (unsigned)px : 0x7fffffffu);
+    const unsigned x1 = __reduce_max_sync(kFull, on ? (unsigned)px : 0u);
+    const unsigned y0 = __reduce_min_sync(kFull, on ? (unsigned)py : 0x7fffffffu);
+    const unsigned y1 = __reduce_max_sync(kFull, on ? (unsigned)py : 0u);
+    // the active segments along the axis (t along a unit ray direction d is t (ax . d) along the axis)
+    const float iW = 1.f / (float)cam.width, iH = 1.f / (float)cam.height;
+    const float lo = jitter == 1 ? 0.333333f : 0.5f, hi = jitter == 1 ? 0.666667f : 0.5f;
+    const float u0 = ((float)x0 + lo) * iW, u1 = ((float)x1 + hi) * iW;
+    const float v0 = ((float)y0 + lo) * iH, v1 = ((float)y1 + hi) * iH;
+    const float3 dc = pixel_dir(cam, 0.5f * (u0 + u1), 0.5f * (v0 + v1));
+    const float3 ax = dc * rsqrtf(dot3(dc, dc));
+    const float cd = dot3(ax, r.d);
+    const float s0 = fmaxf(r.tb * cd, 0.f), s1 = fmaxf(seg_hi * cd, 0.f);
+    const float s_near = __uint_as_float(__reduce_min_sync(kFull, on ? __float_as_uint(s0) : 0x7f800000u));
+    const float s_far = __uint_as_float(__reduce_max_sync(kFull, on ? __float_as_uint(s1) : 0u));
+    if (lane == 0) {
+        const float3 eye = f3(cam.eye[0], cam.eye[1], cam.eye[2]);
+        const float3 U = f3(cam.u[0], cam.u[1], cam.u[2]), V = f3(cam.v[0], cam.v[1], cam.v[2]);
+        const float ae = dot3(ax, eye);
+        const float slack = 2e-5f * (s_far + fabsf(eye.x) + fabsf(eye.y) + fabsf(eye.z) + 1.f);
+        // Side planes through the eye: the rays along a row of sample positions span the camera's
+        // U axis and the row's corner ray, the rays along a column span V and the column's corner
+        // ray, so each side plane holds one camera axis and one corner ray (well conditioned for
+        // any rectangle, a single pixel included).  Inside: towards larger v below the top edge,
+        // smaller v above the bottom edge, and likewise in u.
+        const float3 axis[4] = {U, U, V, V};
+        const float3 corner[4] = {pixel_dir(cam, u0, v0), pixel_dir(cam, u0, v1), pixel_dir(cam, u0, v0),
+                                  pixel_dir(cam, u1, v0)};
+        const float3 toward[4] = {V, V * -1.f, U, U * -1.f};
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+            float3 n = cross3(axis[i], corner[i]);
+            if (dot3(n, toward[i]) < 0.f) n = n * -1.f;
+            n = n * rsqrtf(fmaxf(dot3(n, n), 1e-30f));
+            set_plane(sm.frustum, i, n, dot3(n, eye) - slack);
+        }
+        set_plane(sm.frustum, 4, ax, ae + s_near - slack);
+        set_plane(sm.frustum, 5, ax * -1.f, -(ae + s_far) - slack);
+    }
+    __syncwarp();
+}
+
+// Whether a box meets the beam: for every plane the largest n . x over the box reaches its offset.
+__device__ __forceinline__ bool beam_hit(const float* F, float3 lo, float3 hi) {
+    bool in = true;
+#pragma unroll
+    for (int i = 0; i < kFrustumPlanes; ++i) {
+        const float4 a = *reinterpret_cast<const float4*>(F + 8 * i);
+        const float4 b = *reinterpret_cast<const float4*>(F + 8 * i + 4);
+        const float m = fmaf(a.x, hi.x, fmaf(a.y, hi.y, fmaf(a.z, hi.z, fmaf(a.w, lo.x, fmaf(b.x, lo.y, b.y * lo.z)))));
+        in = in && (m >= b.z);
+    }
+    return in;
 }
 
 __device__ __forceinline__ LeafRec load_rec(const LeafRec* p, int i) {
@@ -408,9 +476,12 @@ __device__ __forceinline__ void finish_list(WarpSmem<FAST, CAP>& sm, int count, 
     __syncwarp();
 }
 
-// Warp-cooperative traversal for the chunk [tb, seg_hi] of every active lane.  Appends hit leaves
-// with index > cursor to the warp list; returns the entry count.  `ovf` is set when the list
-// filled up before the traversal finished.
+// Warp-cooperative traversal for the chunk [tb, seg_hi] of every active lane (the beam set by
+// set_frustum).  At a wide node lane k tests child slot k against the beam; the first hit child is
+// visited next and the others wait on the stack, the lowest index on top, so leaves are reached in
+// increasing index (the multi-pass cursor relies on it).  Appends hit leaves with index > cursor to
+// the warp list; returns the entry count.  `ovf` is set when the list filled up before the
+// traversal finished.
 template <bool FAST, int CAP, bool DIAG>
 __device__ int traverse(WarpSmem<FAST, CAP>& sm, const RenderArgs& a, const RayState& r, bool on, float seg_hi,
                         int K, int nv, int cursor, bool& ovf, int lane, WarpStats& ws, bool infer) {
@@ -421,40 +492,38 @@ __device__ int traverse(WarpSmem<FAST, CAP>& sm, const RenderArgs& a, const RayS
     int sp = 0;
     int cur = (a.n_leaves == 1) ? ~0 : 0;
     unsigned guard = 0, visits = 0;
-    const unsigned guard_max = 4u * (unsigned)a.n_leaves + 64u;
+    const unsigned guard_max = 2u * (unsigned)a.n_leaves + 64u;
     while (true) {
         if (++guard > guard_max) {
             if (lane == 0) atomicAdd(&a.st->watchdog_trips, 1ull);
             break;
         }
         if (cur >= 0) {
-            // 4-wide node: two halves in the binary node format, children in leaf order
             if (DIAG) ++visits;
-            const Node* np = a.nodes4 + 2 * (long long)cur;
-            float ab0[6], ab1[6], bb0[6], bb1[6];
-            int4 na, nb;
-            load_node(np, ab0, ab1, na);
-            load_node(np + 1, bb0, bb1, nb);
-            // non-short-circuit predicates: no branches before the vote
-            const unsigned bits = (unsigned)(box_hit<FAST>(ab0, r, r.tb, seg_hi) & (na.z > cursor)) |
-                                  ((unsigned)(box_hit<FAST>(ab1, r, r.tb, seg_hi) & (na.w > cursor)) << 1) |
-                                  ((unsigned)(box_hit<FAST>(bb0, r, r.tb, seg_hi) & (nb.z > cursor)) << 2) |
-                                  ((unsigned)(box_hit<FAST>(bb1, r, r.tb, seg_hi) & (nb.w > cursor)) << 3);
-            const unsigned hm = __reduce_or_sync(kFull, on ? bits : 0u);
+            const int2 wt = __ldg(a.wide_tab + cur);
+            bool hit = false;
+            int cid = 0;
+            if (lane < wt.y) {
+                float3 lo, hi;
+                int range_hi;
+                load_slot(a.slots + wt.x + lane, lo, hi, cid, range_hi);
+                hit = (range_hi > cursor) && beam_hit(sm.frustum, lo, hi);
+            }
+            const unsigned hm = __ballot_sync(kFull, hit);
             if (hm) {
-                // continue with the first hit child; the later ones wait on the stack, last on
-                // the bottom.  Every lane stores the same value and reads back only its own
-                // stores: the stack needs neither a single writer nor a warp barrier.
+                // continue with the first hit child; the later ones go on the stack in reverse order
+                // (the hit child k at the position of the hit children above it), lowest on top
                 const int f = __ffs(hm) - 1;
-                const int more = __popc(hm) - 1;
-                if (sp + more <= kStack) {
-                    if ((hm & 8u) && f < 3) sm.stack[sp++] = nb.y;
-                    if ((hm & 4u) && f < 2) sm.stack[sp++] = nb.x;
-                    if ((hm & 2u) && f < 1) sm.stack[sp++] = na.y;
+                const unsigned rest = hm & (hm - 1u);
+                const int np = __popc(rest);
+                if (sp + np <= kStack) {
+                    if ((rest >> lane) & 1u) sm.stack[sp + __popc(rest >> lane) - 1] = cid;
+                    sp += np;
                 } else if (lane == 0) {
                     atomicAdd(&a.st->stack_overflows, 1ull);
                 }
-                cur = f == 0 ? na.x : f == 1 ? na.y : f == 2 ? nb.x : nb.y;
+                cur = __shfl_sync(kFull, cid, f);
+                __syncwarp();
                 continue;
             }
         } else {
@@ -977,13 +1046,6 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, min_blocks<BWD, FAST>()) 
             r.tenter = fmaxf(0.f, fmaxf(fminf(t0x, t1x), fmaxf(fminf(t0y, t1y), fminf(t0z, t1z))));
             r.texit = fminf(fmaxf(t0x, t1x), fminf(fmaxf(t0y, t1y), fmaxf(t0z, t1z)));
         }
-        {
-            const float tiny = 1e-20f;
-            r.invd = f3(1.f / (fabsf(r.d.x) > tiny ? r.d.x : copysignf(tiny, r.d.x)),
-                        1.f / (fabsf(r.d.y) > tiny ? r.d.y : copysignf(tiny, r.d.y)),
-                        1.f / (fabsf(r.d.z) > tiny ? r.d.z : copysignf(tiny, r.d.z)));
-            r.oid = f3(-r.o.x * r.invd.x, -r.o.y * r.invd.y, -r.o.z * r.invd.z);
-        }
         r.alive = valid && (r.tenter < r.texit);
         r.tb = r.tenter;
         r.T = 1.f;
@@ -1046,7 +1108,9 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, min_blocks<BWD, FAST>()) 
             }
             bool ovf = false;
             int count;
-            if (BWD && rec_cur != kNoRecord && !(rec_hdr & kRecordMulti)) {
+            const bool replayed = BWD && rec_cur != kNoRecord && !(rec_hdr & kRecordMulti);
+            if (!replayed) set_frustum<FAST, CAP>(sm, a.cams[view], a.jitter, px, py, r, on, seg_hi, lane);
+            if (replayed) {
                 const unsigned n_ids = min(rec_hdr & 0xffffu, a.rec_cap - rec_cur - 2u);
                 count = replay_list<FAST, CAP, DIAG>(sm, a, r, on, seg_hi, K, nv, a.rec_arena + rec_cur + 2, (int)n_ids,
                                                lane, ws);
@@ -1275,6 +1339,13 @@ size_t render_smem_bytes(bool, int cap) {
     return sizeof(WarpSmem<false, 128>) * kWarpsPerBlock;
 }
 static_assert(sizeof(WarpSmem<false, 128>) * kWarpsPerBlock <= 48 * 1024, "static shared memory limit");
+// the beam planes are read as float4: 16-byte aligned in every warp's slice of the block's array
+using ParitySmem = WarpSmem<false, 128>;
+using FastSmem256 = WarpSmem<true, 256>;
+using FastSmem512 = WarpSmem<true, 512>;
+static_assert(offsetof(ParitySmem, frustum) % 16 == 0 && sizeof(ParitySmem) % 16 == 0, "beam plane alignment");
+static_assert(offsetof(FastSmem256, frustum) % 16 == 0 && sizeof(FastSmem256) % 16 == 0, "beam plane alignment");
+static_assert(offsetof(FastSmem512, frustum) % 16 == 0 && sizeof(FastSmem512) % 16 == 0, "beam plane alignment");
 static_assert(sizeof(WarpSmem<true, 512>) * kWarpsPerBlock <= 48 * 1024, "static shared memory limit");
 
 template <bool BWD, bool FAST>
