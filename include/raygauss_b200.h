@@ -253,6 +253,11 @@ RG_API int rg_leaf_order(rg_engine* e, int32_t* leaf_gid_out, void* stream);
  * rg_launch_forward; final_T may be NULL. */
 RG_API int rg_render_forward_noalloc(const rg_gaussians* g, const rg_camera* cams, int32_t n_cams,
                                      const rg_settings* s, float* ray_colors, float* final_T, void* stream);
+/* Device counters of the latest rg_render_forward_noalloc call on the current device (each call
+ * clears them when it starts): synchronises `stream`, then copies the counters out of the static
+ * array, allocating nothing.  record_words is always 0 (the call keeps no hit-list record).  No
+ * counterpart in the reference. */
+RG_API int rg_noalloc_get_status(rg_status* out, void* stream);
 /* Read (and optionally reset) the device counters; synchronises the engine's last stream. */
 RG_API int rg_get_status(rg_engine* e, rg_status* out, int32_t reset, void* stream);
 /* Number of kernels launched by this engine since creation (for launch accounting). */

@@ -152,6 +152,7 @@ SIGNATURES = {
     "rg_leaf_order": (ctypes.c_int, [_P, _P, _P]),
     "rg_render_forward_noalloc": (ctypes.c_int, [ctypes.POINTER(rg_gaussians), _P, ctypes.c_int32,
                                                  ctypes.POINTER(rg_settings), _P, _P, _P]),
+    "rg_noalloc_get_status": (ctypes.c_int, [ctypes.POINTER(rg_status), _P]),
     "rg_train_tail_step": (ctypes.c_int, [ctypes.POINTER(rg_train_tail), _P]),
     "rg_records_to_columns": (ctypes.c_int, [_P, ctypes.c_int64, ctypes.c_int32, ctypes.POINTER(rg_record_field),
                                              ctypes.c_int32, _P]),

@@ -13,6 +13,9 @@
 // array and leaves the previous call's contents in it; each call clears what must start at zero
 // (scene box, refit counters, work counter, status block) on its stream, so calls that overlap on
 // the GPU (different streams, or different host threads without ordering) race on the array.
+// rg_noalloc_get_status reads the device counters of the latest call on the current device
+// (non-finite inputs, watchdog trips, stack overflows and the rest of rg_status), allocating
+// nothing either: it synchronises the given stream and copies the array's status block.
 // The first call on a device looks up the array's device address with cudaGetSymbolAddress and
 // caches it; make that first call before any stream capture.
 #include <cstring>
@@ -32,7 +35,8 @@ constexpr size_t align256(size_t x) { return (x + 255) & ~size_t(255); }
 // Byte offsets of every scratch buffer inside the array.
 struct NoAllocLayout {
     size_t rec, aabb, scene, keys_in, keys_out, vals_in, leaf_gid, rank, leaf_rec, leaf_is, leaf_ext, leaf_lo,
-        leaf_hi, nodes, nodes4, leaf_parent, node_parent, refit_cnt, root_box, rgb_leaf, vt, work, status, sort, total;
+        leaf_hi, nodes, depth, wide_cnt, wide_tab, slots, leaf_parent, node_parent, refit_cnt, root_box, rgb_leaf, vt,
+        work, status, sort, total;
 };
 
 constexpr NoAllocLayout make_layout() {
@@ -58,7 +62,10 @@ constexpr NoAllocLayout make_layout() {
     L.leaf_lo = take(sizeof(float4) * N);
     L.leaf_hi = take(sizeof(float4) * N);
     L.nodes = take(sizeof(rg::Node) * N);
-    L.nodes4 = take(sizeof(rg::Node) * 2 * N);
+    L.depth = take(sizeof(int) * N);
+    L.wide_cnt = take(sizeof(int) * N);
+    L.wide_tab = take(sizeof(int2) * N);
+    L.slots = take(sizeof(rg::WideSlot) * 2 * N);
     L.leaf_parent = take(sizeof(int) * N);
     L.node_parent = take(sizeof(int) * N);
     L.refit_cnt = take(sizeof(unsigned) * N);
@@ -157,7 +164,10 @@ extern "C" RG_API int rg_render_forward_noalloc(const rg_gaussians* g, const rg_
     bvh.leaf_lo = at<float4>(b, kLayout.leaf_lo);
     bvh.leaf_hi = at<float4>(b, kLayout.leaf_hi);
     bvh.nodes = at<rg::Node>(b, kLayout.nodes);
-    bvh.nodes4 = at<rg::Node>(b, kLayout.nodes4);
+    bvh.depth = at<int>(b, kLayout.depth);
+    bvh.wide_cnt = at<int>(b, kLayout.wide_cnt);
+    bvh.wide_tab = at<int2>(b, kLayout.wide_tab);
+    bvh.slots = at<rg::WideSlot>(b, kLayout.slots);
     bvh.leaf_parent = at<int>(b, kLayout.leaf_parent);
     bvh.node_parent = at<int>(b, kLayout.node_parent);
     bvh.refit_cnt = at<unsigned>(b, kLayout.refit_cnt);
@@ -183,7 +193,8 @@ extern "C" RG_API int rg_render_forward_noalloc(const rg_gaussians* g, const rg_
     a.is_rec = bvh.leaf_is;
     a.ext = bvh.leaf_ext;
     a.rgb = rgb_leaf;
-    a.nodes4 = bvh.nodes4;
+    a.wide_tab = bvh.wide_tab;
+    a.slots = bvh.slots;
     a.n_leaves = (int)n;
     a.scene_ord = scene_ord;
     a.white_bg = s->white_background;
@@ -191,14 +202,31 @@ extern "C" RG_API int rg_render_forward_noalloc(const rg_gaussians* g, const rg_
     a.rnd_sample = s->rnd_sample;
     a.max_prim_slice = s->max_prim_slice > 0 ? s->max_prim_slice : 1024;
     a.iteration = s->iteration;
-    a.chunk_slabs = 64;  // the engine's default tuning
+    a.chunk_slabs = 64;  // the engine's default tuning: 64-slab chunks, list capacity 64
     a.work_counter = work;
     a.st = status;
     a.ray_colors = ray_colors;
     a.final_T = final_T;
-    const int cap = 128;
-    int per_sm = rg::render_occupancy(false, s->mode, cap);
+    const int cap = 64;
+    // random sample offsets run the parity kernel in either mode (launch_render picks it): size the
+    // grid for the kernel that runs
+    const int run_mode = (s->mode == RG_MODE_FAST && s->rnd_sample == 0) ? RG_MODE_FAST : RG_MODE_PARITY;
+    int per_sm = rg::render_occupancy(false, run_mode, cap);
     int grid = d->num_sms * (per_sm > 0 ? per_sm : 1);
     if (rg::launch_render(false, s->mode, cap, grid, a, st) != cudaSuccess) return RG_ERR_CUDA;
+    return RG_OK;
+}
+
+extern "C" RG_API int rg_noalloc_get_status(rg_status* out, void* stream) {
+    if (!out) return RG_ERR_INVALID_ARG;
+    int dev = -1;
+    if (cudaGetDevice(&dev) != cudaSuccess) return RG_ERR_CUDA;
+    DeviceSetup* d = nullptr;
+    int rc = setup_device(dev, &d);
+    if (rc) return rc;
+    if (cudaStreamSynchronize(reinterpret_cast<cudaStream_t>(stream)) != cudaSuccess) return RG_ERR_CUDA;
+    rg::DevStatus h;
+    if (cudaMemcpy(&h, d->base + kLayout.status, sizeof(h), cudaMemcpyDeviceToHost) != cudaSuccess) return RG_ERR_CUDA;
+    rg::export_status(h, out);
     return RG_OK;
 }

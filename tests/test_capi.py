@@ -78,6 +78,8 @@ def test_invalid_arguments_rejected_without_gpu(engine_lib):
     assert engine_lib.rg_launch_forward(None, None, 1, None, None, None, None) == 1
     st = _lib.rg_status()
     assert engine_lib.rg_get_status(None, ctypes.byref(st), 0, None) == 1
+    assert engine_lib.rg_noalloc_get_status(None, None) == 1
+    assert engine_lib.rg_render_forward_noalloc(None, None, 1, None, None, None, None) == 1
     assert engine_lib.rg_destroy(None) == 0
 
 
