@@ -132,16 +132,61 @@ def main():
     ap.add_argument("--n", type=int, default=1_000_000)
     ap.add_argument("--no-plain", action="store_true", help="skip the plain single-view comparison")
     ap.add_argument("--no-cpu", action="store_true", help="skip the host-core baseline")
-    ap.add_argument("--cpu-rays", type=int, default=256, help="rays per view in the host-core sample")
+    ap.add_argument("--cpu-rays", type=int, default=4096, help="rays per view in the accuracy and host-core samples")
     ap.add_argument("--no-tune", action="store_true", help="skip the autotuner (engine defaults)")
     ap.add_argument("--no-graph", action="store_true", help="skip the CUDA-graph replay measurement")
+    ap.add_argument("--plain-only", action="store_true",
+                    help="run only the plain drop-in form (RenderOptixFunction per view, parity arithmetic) for "
+                         "--steps steps and print its Mrays/s (a profiling case for its kernels)")
+    ap.add_argument("--drift", type=int, default=0,
+                    help="also measure refit-only LBVH drift over this many captured training iterations")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
     rank, world, local = _dist()
     if args.impl == "reference":
         return reference_arm(args, rank, world)
+    if args.plain_only:
+        return plain_only(args, local)
     return our_arm(args, rank, world, local)
+
+
+def plain_only(args, local):
+    """The plain FP32 drop-in form alone: RenderOptixFunction forward + MSE + backward per view."""
+    import torch
+    from ray_gauss_b200.engine import Engine
+    from ray_gauss_b200.optix_raycasting.render_optix import RenderOptixFunction, RenderOptixSettings
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    _, P32, cams, white = _setup(args, dev)
+    P = {k: v.clone().requires_grad_(True) for k, v in P32.items()}
+    nsg = P["sph_gauss_features"].shape[2]
+    eng = Engine(local)
+    targets = [torch.rand((c.image_width * c.image_height, 3), device=dev) for c in cams]
+
+    def step():
+        for v, cam in enumerate(cams):
+            s = RenderOptixSettings(eng, False, None, None, None, None, None, cam, 1024, nsg, 0, 0, 0, (1, 1), white,
+                                    None, mode="parity")
+            img = RenderOptixFunction.apply(*(P[k] for k in GRAD_KEYS), s)
+            torch.nn.functional.mse_loss(img, targets[v]).backward()
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(args.steps):
+        step()
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / args.steps
+    R = sum(c.image_width * c.image_height for c in cams)
+    print(json.dumps({"form": "plain FP32 drop-in (RenderOptixFunction per view, parity arithmetic)",
+                      "gaussians": int(P32["positions"].shape[0]), "views": len(cams), "rays_per_step": R,
+                      "ms_per_step": round(ms, 3), "value": round(R / (ms * 1e-3) / 1e6, 3), "unit": "Mrays/s"}))
+    return 0
 
 
 def _setup(args, device):
@@ -247,7 +292,7 @@ def our_arm(args, rank, world, local):
     ms_max = max_over_ranks(ms, dev)
     value = world * R / (ms_max * 1e-3) / 1e6
 
-    # dominant kernel: the backward launch (events on the launching stream)
+    # render launches (CUDA events on the launching stream, averaged over the timed steps)
     bwd_ms = statistics.mean(a.elapsed_time(b) for a, b in timers["launch_backward"])
     fwd_ms = statistics.mean(a.elapsed_time(b) for a, b in timers["launch_forward"])
     prep_ms = statistics.mean(a.elapsed_time(b) for a, b in timers["prepare"])
@@ -255,29 +300,46 @@ def our_arm(args, rank, world, local):
     nsg = P32["sph_gauss_features"].shape[2]
     ncoef = P32["color_features"].shape[2]
     V = len(cams)
-    # algorithmic bytes of one backward launch: leaf records (64 B) + scale/quaternion (32 B) + colour per
-    # view (16 B) read once per Gaussian, gradient accumulators written once (48 B + 16 B per view), ray
-    # colour and dL/dcolour read once per ray (24 B)
-    # plus the forward's hit-list record, read once (4 B per recorded word)
-    rec_bytes = 4 * st.get("record_words", 0)   # size of the last forward's record (not a running sum)
-    alg_bwd = n * (64 + 32 + 16 * V) + n * (48 + 16 * V) + 24 * R + rec_bytes
-    peak, peak_kind = _peaks()
-    achieved = alg_bwd / (bwd_ms * 1e-3) / 1e9
-    # DRAM traffic and SM issue utilisation of this launch from the committed ncu summary of the same
-    # workload (a profiler number is never timed here)
-    prof = _profile_figures(TRAFFIC_PROFILE)
-    traffic = None
-    if prof.get("gaussians") == n and prof.get("views") == V and "backward_dram_bytes" in prof:
-        traffic = int(prof["backward_dram_bytes"])
-    roofline = {"bound": "hbm", "achieved": round(achieved, 2), "peak": peak, "unit": "GB/s",
-                "frac": round(achieved / peak, 5), "traffic": traffic, "peak_source": peak_kind,
-                "kernel": "k_render<backward> (rg_launch_backward)",
-                "algorithmic_bytes_per_launch": int(alg_bwd),
-                "sm_issue_frac_ncu": prof.get("backward_sm_issue_frac"),
-                "note": "L2-resident gather/accumulate: bound by SM instruction issue, not HBM"}
-    # step-level algorithmic bytes (parameters read twice, gradients written once, 36 B per ray)
     p_store = bytes_per_gaussian(nsg, ncoef, True)
     g_bytes = bytes_per_gaussian(nsg, ncoef, False)
+    # algorithmic bytes per launch (parameters counted once per launch, all views):
+    #   forward  B_fwd = N P_store + 12 R (parameters read once, ray colours written)
+    #   backward the leaf records (64 B) + scale/quaternion (32 B) + colour per view (16 B) read once per
+    #            Gaussian, the gradient accumulators written once (48 B + 16 B per view), ray colour and
+    #            dL/dcolour read once per ray (24 B), and the forward's hit-list record read once
+    rec_bytes = 4 * st.get("record_words", 0)   # size of the last forward's record (not a running sum)
+    alg_fwd = n * p_store + 12 * R
+    alg_bwd = n * (64 + 32 + 16 * V) + n * (48 + 16 * V) + 24 * R + rec_bytes
+    peak, peak_kind = _peaks()
+    # DRAM traffic and SM issue utilisation from the committed ncu summary of the same workload (a
+    # profiler number is never timed here)
+    prof = _profile_figures(TRAFFIC_PROFILE)
+    same = prof.get("gaussians") == n and prof.get("views") == V
+    hit_pairs = st.get("hit_pairs", 0) / max(1, args.steps)   # forward + backward recompute, per step
+    rl_launches = {}
+    for name, ms_l, alg in (("forward", fwd_ms, alg_fwd), ("backward", bwd_ms, alg_bwd)):
+        ach = alg / (ms_l * 1e-3) / 1e9
+        traffic = int(prof[f"{name}_dram_bytes"]) if same and f"{name}_dram_bytes" in prof else None
+        rl_launches[name] = {
+            "kernel": f"k_render<{name}> (rg_launch_{name})", "ms_per_launch": round(ms_l, 3),
+            "algorithmic_bytes_per_launch": int(alg), "achieved_gbs": round(ach, 2), "frac": round(ach / peak, 6),
+            "traffic": traffic, "traffic_over_algorithmic": round(traffic / alg, 3) if traffic else None,
+            "sm_issue_frac_ncu": prof.get(f"{name}_sm_issue_frac"),
+            # each (ray, slab, Gaussian) pair evaluates 8 samples in the forward and again in the backward
+            "g_hit_samples_per_s": round(8 * hit_pairs / 2 / (ms_l * 1e-3) / 1e9, 3)}
+    dom = "forward" if fwd_ms >= bwd_ms else "backward"
+    d = rl_launches[dom]
+    roofline = {"bound": "hbm", "achieved": d["achieved_gbs"], "peak": peak, "unit": "GB/s", "frac": d["frac"],
+                "traffic": d["traffic"], "peak_source": peak_kind, "kernel": d["kernel"],
+                "algorithmic_bytes_per_launch": d["algorithmic_bytes_per_launch"],
+                "traffic_over_algorithmic": d["traffic_over_algorithmic"],
+                "sm_issue_frac_ncu": d["sm_issue_frac_ncu"], "launches": rl_launches,
+                "note": "the dominant launch is the longer of the two render launches; both are bound by SM "
+                        "instruction issue (gathers of L2-resident Gaussian records, FP32 and SFU sample math), "
+                        "not by HBM: the HBM fraction is small by construction and sm_issue_frac_ncu is the "
+                        "compute-side figure; traffic above the algorithmic bytes is the forward's hit-list "
+                        "record and per-view colour tables"}
+    # step-level algorithmic bytes (parameters read twice, gradients written once, 36 B per ray)
     b_step = 2 * n * p_store + n * g_bytes + 36 * R
 
     # ---- the same step captured as one CUDA graph (refit + forward + loss + backward) ----
@@ -527,11 +589,89 @@ def our_arm(args, rank, world, local):
         plain = {"value": round(R / (p_ms * 1e-3) / 1e6, 3), "unit": "Mrays/s", "ms_per_step": round(p_ms, 3),
                  "form": "RenderOptixFunction per view, FP32 storage, parity arithmetic"}
 
+    # ---- attribution of batched_over_plain: arithmetic, storage and batching one at a time ----
+    attribution = None
+    bounded = None
+    if not args.no_plain:
+        tviews = [target[views.offsets[v]:views.offsets[v + 1]] for v in range(V)]
+
+        def per_view_step(P, mode):
+            def run():
+                for v, cam in enumerate(cams):
+                    s = RenderOptixSettings(eng, False, None, None, None, None, None, cam, 1024, nsg, 0, 0, 0,
+                                            (1, 1), white, None, mode=mode)
+                    img = RenderOptixFunction.apply(*(P[k] for k in GRAD_KEYS), s)
+                    torch.nn.functional.mse_loss(img, tviews[v]).backward()
+            return run
+
+        def batched_step(P, bviews, tgt):
+            def run():
+                out = BatchedRenderFunction.apply(*(P[k] for k in GRAD_KEYS), bviews)
+                torch.nn.functional.mse_loss(out, tgt).backward()
+            return run
+
+        def timed(run, P, reps):
+            zero(P)
+            run()
+            torch.cuda.synchronize()
+            a0 = torch.cuda.Event(enable_timing=True)
+            a1 = torch.cuda.Event(enable_timing=True)
+            a0.record()
+            for _ in range(reps):
+                zero(P)
+                run()
+            a1.record()
+            torch.cuda.synchronize()
+            return a0.elapsed_time(a1) / reps
+
+        reps = max(1, args.steps // 2)
+        L32 = {k: v.clone().requires_grad_(True) for k, v in P32.items()}
+        Lb = {k: v.clone().requires_grad_(True) for k, v in Pb.items()}
+        bviews32 = BatchedViews(cams, white_background=white, mode="fast", engine=eng)
+        legs = [("single_view_parity_fp32", per_view_step(L32, "parity"), L32),
+                ("single_view_fast_fp32", per_view_step(L32, "fast"), L32),
+                ("single_view_fast_bf16", per_view_step(Lb, "fast"), Lb),
+                ("batched_fast_fp32", batched_step(L32, bviews32, target), L32),
+                ("batched_fast_bf16", batched_step(Lb, views, target), Lb)]
+        attribution = {}
+        for name, run, P in legs:
+            a_ms = timed(run, P, reps)
+            attribution[name] = {"value": round(R / (a_ms * 1e-3) / 1e6, 3), "unit": "Mrays/s",
+                                 "ms_per_step": round(a_ms, 3)}
+        attribution["note"] = ("fwd+bwd of the same 16 views, one factor changed per line: arithmetic (parity -> "
+                               "fast), storage (FP32 -> BF16), launch (one view per launch -> all views in one "
+                               "launch)")
+        del L32, Lb, bviews32
+
+        # ---- the bounded-object configuration: 300k Gaussians on shells, SH3 + 8 SG, one 800x800 view ----
+        from ray_gauss_b200 import synthetic as S
+        pb, bcams, bwhite = S.workload("bounded_object", seed=0, device="cpu")
+        bcam = bcams[0].to(dev)
+        B32 = {k: v.to(dev).requires_grad_(True) for k, v in pb.items()}
+        Bb = _bf16({k: v.detach() for k, v in B32.items()})
+        Bb = {k: v.clone().requires_grad_(True) for k, v in Bb.items()}
+        bR = bcam.image_width * bcam.image_height
+        btgt = torch.rand((bR, 3), device=dev, generator=torch.Generator(device=dev).manual_seed(3))
+        bounded = {"workload": "bounded_object: 300k Gaussians on 8 seeded shells, SH3 + 8 SG, one 800x800 view, "
+                               "white background", "rays_per_step": bR}
+        for name, P, mode in (("parity_fp32", B32, "parity"), ("fast_fp32", B32, "fast"), ("fast_bf16", Bb, "fast")):
+            def run(P=P, mode=mode):
+                s = RenderOptixSettings(eng, False, None, None, None, None, None, bcam, 1024, 8, 0, 0, 0, (1, 1),
+                                        bwhite, None, mode=mode)
+                img = RenderOptixFunction.apply(*(P[k] for k in GRAD_KEYS), s)
+                torch.nn.functional.mse_loss(img, btgt).backward()
+            b_ms = timed(run, P, max(2, args.steps))
+            bounded[name] = {"value": round(bR / (b_ms * 1e-3) / 1e6, 3), "unit": "Mrays/s",
+                             "ms_per_step": round(b_ms, 3)}
+        del B32, Bb
+
     # ---- accuracy of the headline form: PSNR against the FP64 oracle on 64x64 crops (reported) ----
     accuracy = None
     cpu_baseline = None
     if rank == 0 and not args.no_cpu:
         accuracy, cpu_baseline = _host_side(args, p_host, cams, white, views, leaves, Pb, eng)
+
+    drift = _drift_leg(args, dev) if args.drift > 0 and rank == 0 else None
 
     if world > 1:
         import torch.distributed as dist
@@ -567,7 +707,10 @@ def our_arm(args, rank, world, local):
         "inference": inference,
         "plain_fp32_single_view": plain,
         "batched_over_plain": round(value / world / plain["value"], 3) if plain else None,
+        "batched_over_plain_attribution": attribution,
+        "bounded_object": bounded,
         "accuracy": accuracy,
+        "refit_drift": drift,
         "cpu_baseline": cpu_baseline,
         "clocks": clk,
     }
@@ -575,50 +718,206 @@ def our_arm(args, rank, world, local):
     return 0
 
 
+def _drift_leg(args, dev):
+    """Refit-only LBVH drift: the captured training iteration (GraphedStep with the fused Adam tail,
+    the reference's base learning rates, positions scaled by the cameras' extent as in
+    scripts/train.py:46-47) refits the tree built at capture time, while the reference rebuilds its
+    GAS every iteration.  At a few iterations, the forward's node visits and time on the refitted
+    tree are compared with those on a tree rebuilt from the same parameters (a second engine)."""
+    import torch
+    from ray_gauss_b200 import synthetic as S
+    from ray_gauss_b200.batched import BatchedRenderFunction, BatchedViews
+    from ray_gauss_b200.engine import Engine
+    from ray_gauss_b200.graph import GraphedStep
+    from ray_gauss_b200.train_tail import FusedTrainTail, LrSchedule, point_cloud_data, raw_from_render_inputs
+    p, cams, white = S.workload(WORKLOAD, seed=0, device="cpu", n=args.n)
+    cams = [c.to(dev) for c in cams[:4]]
+    centres = np.stack([c.camera_center.cpu().numpy() for c in cams])
+    extent = 1.1 * float(np.linalg.norm(centres - centres.mean(0), axis=1).max())
+    raw = {k: v.to(dev).contiguous() for k, v in raw_from_render_inputs({k: v for k, v in p.items()}).items()}
+    trained = {k: v for k, v in raw.items() if v.numel()}
+    exp = LrSchedule.exponential
+    sched = {"positions": exp(1.7e-5 * extent, 1e-6 * extent, 30000), "densities": exp(0.5, 1e-4, 30000),
+             "rgb": LrSchedule(1e-3), "spherical_harmonics": LrSchedule(2.6e-4), "scales": LrSchedule(0.0115),
+             "quaternions": LrSchedule(2.2e-4), "sph_gauss_features": LrSchedule(3.6e-4),
+             "bandwidth_sharpness": LrSchedule(0.045), "lobe_axis": LrSchedule(0.003)}
+    tail = FusedTrainTail(trained, {k: sched[k] for k in trained},
+                          roles={"positions": "positions", "densities": "densities", "scales": "scales",
+                                 "quaternions": "quaternions"})
+    eng = Engine(dev.index or 0)
+    views = BatchedViews(cams, white_background=white, mode="fast", engine=eng)
+    target = torch.rand((views.n_rays, 3), device=dev, generator=torch.Generator(device=dev).manual_seed(9))
+    act = lambda r: point_cloud_data(r, normalized_quaternion=False)  # noqa: E731
+    step = GraphedStep(raw, views, target, tail=tail, min_scale=torch.full((raw["positions"].shape[0],), -12.0,
+                                                                             device=dev), activation=act)
+    fresh = Engine(dev.index or 0)
+    fviews = BatchedViews(cams, white_background=white, mode="fast", engine=fresh)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+
+    def forward_stats(e, v, refit):
+        v.update = refit
+        e.set_tuning(diagnostics=1)
+        e.status(reset=True)
+        with torch.no_grad():
+            X = act(raw)
+            BatchedRenderFunction.apply(*(X[k] for k in GRAD_KEYS), v)
+        torch.cuda.synchronize()
+        visits = e.status(reset=True)["node_visits"]
+        e.set_tuning(diagnostics=0)
+        with torch.no_grad():
+            X = act(raw)
+            e0.record()
+            BatchedRenderFunction.apply(*(X[k] for k in GRAD_KEYS), v)
+            e1.record()
+        torch.cuda.synchronize()
+        return int(visits), round(e0.elapsed_time(e1), 3)
+
+    marks = sorted({1, max(1, args.drift // 3), args.drift})
+    out = {"iterations": args.drift, "views": len(cams), "gaussians": int(raw["positions"].shape[0]),
+           "cameras_extent": round(extent, 3), "points": []}
+    done = 0
+    for m in marks:
+        while done < m:
+            step.replay()
+            done += 1
+        torch.cuda.synchronize()
+        e0.record()
+        for _ in range(3):
+            step.replay()
+        e1.record()
+        torch.cuda.synchronize()
+        done += 3
+        replay_ms = e0.elapsed_time(e1) / 3
+        v_refit, f_refit = forward_stats(eng, views, True)
+        v_build, f_build = forward_stats(fresh, fviews, False)
+        out["points"].append({"iteration": done, "replay_ms": round(replay_ms, 3),
+                              "forward_node_visits_refit": v_refit, "forward_node_visits_rebuilt": v_build,
+                              "visits_refit_over_rebuilt": round(v_refit / max(1, v_build), 4),
+                              "forward_ms_refit": f_refit, "forward_ms_rebuilt": f_build})
+    views.update = False
+    return out
+
+
+def _cpu_model():
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
+GRAD_KEYS = ("positions", "scales", "quaternions", "densities", "color_features", "sph_gauss_features",
+             "bandwidth_sharpness", "lobe_axis")
+
+
+def _oracle_rays(O, P, cv, W, H, white, ids, dL, prec):
+    """Oracle image of the rays `ids` of one view and every parameter gradient of sum(image * dL)."""
+    rgb = O.forward_sh(cv[:3], P["positions"], P["color_features"], P["sph_gauss_features"],
+                       P["bandwidth_sharpness"], P["lobe_axis"], prec=prec)
+    aabb, box = O.bbox(P["positions"], P["scales"], P["quaternions"], P["densities"], prec)
+    img, _, _ = O.render_forward(P["positions"], P["scales"], P["quaternions"], P["densities"], rgb, cv, W, H, white,
+                                 ray_ids=ids, aabb=aabb, scene_box=box, prec=prec)
+    g = O.render_backward(P["positions"], P["scales"], P["quaternions"], P["densities"], rgb, cv, W, H, img, dL,
+                          ray_ids=ids, aabb=aabb, scene_box=box, prec=prec)
+    dt = np.float64 if prec == "f64" else np.float32
+    dsh, dpos, dsg, dkap, dax = O.backward_sh(cv[:3], P["positions"], P["color_features"], P["sph_gauss_features"],
+                                              P["bandwidth_sharpness"], P["lobe_axis"], g["d_rgb"].astype(dt),
+                                              prec=prec, ref_quirks=True)
+    grads = dict(positions=g["d_pos"] + dpos, scales=g["d_scl"], quaternions=g["d_quat"], densities=g["d_dens"],
+                 color_features=dsh, sph_gauss_features=dsg, bandwidth_sharpness=dkap, lobe_axis=dax)
+    return img, grads
+
+
+def _rel_l2(a, b):
+    a = np.asarray(a, np.float64).ravel()
+    b = np.asarray(b, np.float64).ravel()
+    nb = np.linalg.norm(b)
+    return float(np.linalg.norm(a - b) / (nb if nb > 0 else 1.0))
+
+
+def _psnr(a, b):
+    mse = float(np.mean((np.asarray(a, np.float64) - np.asarray(b, np.float64)) ** 2))
+    return 99.0 if mse == 0 else round(-10 * math.log10(mse), 2)
+
+
 def _host_side(args, p_host, cams, white, views, leaves, Pb, eng):
-    """PSNR of the headline form against the FP64 oracle on seeded 64x64 crops, and the host-core baseline."""
+    """Accuracy of the benchmarked form against the FP64 oracle, and the host-core baseline.
+
+    Rays: 4096 seeded random rays of each of views 0 and 1.  The headline form (BF16 storage, fast
+    arithmetic, all views in one launch) renders the whole batch; the loss gradient is non-zero only
+    on the sampled rays, so its FP32 parameter gradients (read from the engine, before autograd
+    casts them to the BF16 leaves' dtype) are sums over those rays and the oracle computes them from
+    the same rays.  References: the FP64 oracle of the BF16-rounded parameters (the arithmetic's
+    error) and of the FP32 parameters (storage rounding included).  The baseline times the FP32 C
+    restatement, with its grid candidate prefilter, over the same rays on all host cores."""
     import torch
     from oracle import oracle as O
+    from ray_gauss_b200 import _lib
+    from ray_gauss_b200.engine import make_gaussians, settings_struct
     rng = np.random.default_rng(7)
-    n = p_host["positions"].shape[0]
-    # one rendered batch of the headline form (already computed in the timed loop; re-render once)
+    V = len(cams)
+    n_views = min(2, V)
+    rays = args.cpu_rays
+    R = views.n_rays
+    ids = []
+    for v in range(n_views):
+        W, H = cams[v].image_width, cams[v].image_height
+        ids.append(np.sort(rng.choice(W * H, min(rays, W * H), replace=False)).astype(np.int32))
+    dLs = [rng.normal(0.0, 1e-3, (len(i), 3)).astype(np.float32) for i in ids]
+    # the benchmarked form through the engine: FP32 gradients of the sampled rays' loss
+    g = make_gaussians(*(Pb[k] for k in GRAD_KEYS))
+    cams_t, _, _ = eng.cameras(views.cameras, views.supersampling)
+    st = settings_struct(white, mode=_lib.RG_MODE_FAST)
     with torch.no_grad():
-        from ray_gauss_b200.batched import BatchedRenderFunction
-        out = BatchedRenderFunction.apply(*(Pb[k] for k in ("positions", "scales", "quaternions", "densities",
-                                                            "color_features", "sph_gauss_features",
-                                                            "bandwidth_sharpness", "lobe_axis")), views)
-    imgs = views.split(out.float().cpu())
-    Pn = {k: v.float().cpu().numpy() for k, v in Pb.items()}
-    acc = []
+        out, _ = eng.render_forward(g, cams_t, V, R, st)
+        dL = torch.zeros((R, 3), dtype=torch.float32, device=out.device)
+        for v in range(n_views):
+            idx = torch.from_numpy(ids[v].astype(np.int64) + int(views.offsets[v])).to(out.device)
+            dL[idx] = torch.from_numpy(dLs[v]).to(out.device)
+        gr = eng.render_backward(g, cams_t, V, st, out, dL)
+        torch.cuda.synchronize()
+    gpu_img = out.cpu().numpy()
+    gpu_g = {k: gr[k].cpu().numpy() for k in GRAD_KEYS}
+    P_round = {k: v.double().cpu().numpy() for k, v in Pb.items()}                 # BF16-rounded
+    P_full = {k: np.asarray(v, np.float64) for k, v in p_host.items()}              # FP32 parameters
+    P32 = {k: np.asarray(v, np.float32) for k, v in p_host.items()}
+    acc = {"rays_per_view": int(rays), "views": n_views, "form": "BF16 storage, fast arithmetic, batched launch",
+           "images": []}
+    sums = {"round": {k: 0.0 for k in GRAD_KEYS}, "full": {k: 0.0 for k in GRAD_KEYS}}
     t_cpu, rays_cpu = 0.0, 0
-    threads = O.num_threads()
-    for v in range(min(2, len(cams))):
+    for v in range(n_views):
         cam = cams[v]
         W, H = cam.image_width, cam.image_height
         cv = O.camera_vector(cam)
-        rgb = O.forward_sh(cv[:3], Pn["positions"], Pn["color_features"], Pn["sph_gauss_features"],
-                           Pn["bandwidth_sharpness"], Pn["lobe_axis"])
-        aabb, box = O.bbox(Pn["positions"], Pn["scales"], Pn["quaternions"], Pn["densities"], "f32")
-        x0, y0 = int(rng.integers(0, W - 64)), int(rng.integers(0, H - 64))
-        ids = np.array([(y0 + j) * W + (x0 + i) for j in range(64) for i in range(64)], np.int32)
-        ids = ids[:: max(1, len(ids) // args.cpu_rays)][: args.cpu_rays]
+        img_r, g_r = _oracle_rays(O, P_round, cv, W, H, white, ids[v], dLs[v], "f64")
+        img_f, g_f = _oracle_rays(O, P_full, cv, W, H, white, ids[v], dLs[v], "f64")
+        for k in GRAD_KEYS:
+            sums["round"][k] = sums["round"][k] + g_r[k]
+            sums["full"][k] = sums["full"][k] + g_f[k]
+        gi = gpu_img[int(views.offsets[v]) + ids[v]]
+        acc["images"].append({"view": v, "psnr_vs_fp64_of_bf16_params_db": _psnr(gi, img_r),
+                              "max_abs_vs_fp64_of_bf16_params": float(np.abs(gi - img_r).max()),
+                              "psnr_vs_fp64_of_fp32_params_db": _psnr(gi, img_f),
+                              "max_abs_vs_fp64_of_fp32_params": float(np.abs(gi - img_f).max())})
+        # host-core baseline: the FP32 restatement over the same rays (grid build included)
         t = time.perf_counter()
-        img32, _, _ = O.render_forward(Pn["positions"], Pn["scales"], Pn["quaternions"], Pn["densities"], rgb, cv, W,
-                                       H, white, ray_ids=ids, aabb=aabb, scene_box=box, prec="f32")
-        dL = np.full(img32.shape, 1e-3, np.float32)
-        O.render_backward(Pn["positions"], Pn["scales"], Pn["quaternions"], Pn["densities"], rgb, cv, W, H, img32, dL,
-                          ray_ids=ids, aabb=aabb, scene_box=box, prec="f32")
+        _oracle_rays(O, P32, cv, W, H, white, ids[v], dLs[v], "f32")
         t_cpu += time.perf_counter() - t
-        rays_cpu += len(ids)
-        img64, _, _ = O.render_forward(Pn["positions"], Pn["scales"], Pn["quaternions"], Pn["densities"], rgb, cv, W,
-                                       H, white, ray_ids=ids, prec="f64")
-        gpu = imgs[v].reshape(-1, 3).numpy()[ids]
-        mse = float(np.mean((gpu.astype(np.float64) - img64) ** 2))
-        acc.append({"view": v, "psnr_vs_fp64_oracle_db": (99.0 if mse == 0 else round(-10 * math.log10(mse), 2)),
-                    "max_abs": float(np.abs(gpu - img64).max()), "rays": int(len(ids))})
+        rays_cpu += len(ids[v])
+    acc["grad_rel_l2_vs_fp64_of_bf16_params"] = {k: _rel_l2(gpu_g[k], sums["round"][k]) for k in GRAD_KEYS}
+    acc["grad_rel_l2_vs_fp64_of_fp32_params"] = {k: _rel_l2(gpu_g[k], sums["full"][k]) for k in GRAD_KEYS}
+    acc["grad_rel_l2_max_vs_fp64_of_bf16_params"] = max(acc["grad_rel_l2_vs_fp64_of_bf16_params"].values())
+    threads = O.num_threads()
     cpu = {"value": round(rays_cpu / t_cpu / 1e6, 6), "unit": "Mrays/s", "cores": threads, "kind": "port",
-           "sample": f"{rays_cpu} rays from seeded 64x64 crops of {min(2, len(cams))} views, FP32 forward+backward "
-                     "with the C restatement (brute-force candidate list per ray)"}
+           "cpu_model": _cpu_model(),
+           "sample": f"{rays_cpu} seeded random rays ({rays} per view, views 0-{n_views - 1}) of the 1M-Gaussian "
+                     "workload, FP32 forward+backward (SH/SG, bbox, render, adjoint) with the C restatement on "
+                     f"{threads} OpenMP threads; ray candidates from a nested uniform grid over the AABBs (built "
+                     "per call, included) and a per-ray slab sweep"}
     return acc, cpu
 
 
@@ -636,7 +935,7 @@ def reference_arm(args, rank, world):
     Pn = {k: v.numpy().astype(np.float32) for k, v in p.items()}
     use_ref = O.ref_available()
     rng = np.random.default_rng(3)
-    rays = max(8, args.cpu_rays // 8) if use_ref else max(16, args.cpu_rays // 4)
+    rays = max(64, args.cpu_rays // 2)   # per step: about 2-4 s on 8-16 host cores
     prepared = []
     for cam in cams[:2]:
         cv = O.camera_vector(cam)
@@ -668,15 +967,18 @@ def reference_arm(args, rank, world):
     ms = statistics.mean(times) * 1e3
     value = rays / (ms * 1e-3) / 1e6
     kind = "reference" if use_ref else "port"
-    what = ("the reference's training device programs compiled for the CPU (oracle/_ref; OptiX traversal "
-            "emulated by a per-ray candidate list)" if use_ref else "the C restatement (oracle/liboracle.so)")
+    what = ("the reference's training device programs compiled for the CPU (oracle/_ref); each optixTrace "
+            "call finds its primitives through a nested uniform grid over the AABBs, built per launch like the "
+            "reference's per-iteration GAS build" if use_ref else
+            "the C restatement (oracle/liboracle.so) with its grid candidate prefilter")
     line = {"impl": "reference", "metric": METRIC, "value": round(value, 6), "unit": "Mrays/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms, 3), "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "config": {"workload": f"{WORKLOAD}: {args.n} Gaussians, views 0-1, {rays} random rays per step, "
                                    "FP32 forward+backward on host cores"},
             "cpu_baseline": {"value": round(value, 6), "unit": "Mrays/s", "cores": O.num_threads(), "kind": kind,
-                             "sample": f"{rays} random rays of views 0/1 per step, forward+backward, {what}"},
+                             "cpu_model": _cpu_model(),
+                             "sample": f"{rays} random rays of view 0 or 1 per step, forward+backward, {what}"},
             "e2e": {"value": round(value, 6), "unit": "Mrays/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line))
     return 0
