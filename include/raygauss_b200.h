@@ -102,7 +102,7 @@ typedef struct rg_gaussians {
     const void* sph_gauss_features;    /* (N,3,nsg), f32 or bf16; may be NULL when nsg == 0 */
     const float* bandwidth_sharpness;  /* (N,nsg) after softplus; may be NULL when nsg == 0 */
     const float* lobe_axis;            /* (N,nsg,3) unit axes; may be NULL when nsg == 0 */
-    int64_t n;
+    int64_t n;                         /* 1 .. 2^25 (33,554,432) Gaussians per engine */
     int32_t sh_degree;                 /* 0..3 */
     int32_t num_sph_gauss;             /* 0..RG_MAX_SG */
     int32_t storage;                   /* enum rg_storage */

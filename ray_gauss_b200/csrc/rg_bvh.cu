@@ -325,8 +325,14 @@ __global__ void k_wide_fill(int n, const Node* __restrict__ nodes, const int2* _
     wide_frontier(nodes, i, [&](int k, int id, const float* b) {
         WideSlot sl;
         for (int a = 0; a < 3; ++a) { sl.lo[a] = b[a]; sl.hi[a] = b[3 + a]; }
-        sl.id = id;
-        sl.range_hi = id < 0 ? ~id : nodes[id].n3.w;
+        if (id < 0) {
+            sl.id = id;
+            sl.range_hi = ~id;
+        } else {
+            const int2 c = tab[id];
+            sl.id = wide_pack(c.x, c.y);
+            sl.range_hi = nodes[id].n3.w;
+        }
         out[k] = sl;
     });
 }

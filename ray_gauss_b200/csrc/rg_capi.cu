@@ -144,7 +144,7 @@ int ensure_record(rg_engine* e, long long n_rays) {
 
 int check_gaussians(const rg_gaussians* g) {
     if (!g || !g->positions || !g->scales || !g->quaternions || !g->densities || !g->color_features) return RG_ERR_INVALID_ARG;
-    if (g->n <= 0 || g->n >= (long long)INT_MAX) return RG_ERR_INVALID_ARG;
+    if (g->n <= 0 || g->n > rg::kMaxGaussians) return RG_ERR_INVALID_ARG;   // wide-node slot ids: 2^25
     if (g->sh_degree < 0 || g->sh_degree > 3) return RG_ERR_INVALID_ARG;
     if (g->num_sph_gauss < 0 || g->num_sph_gauss > RG_MAX_SG) return RG_ERR_INVALID_ARG;
     if (g->num_sph_gauss > 0 && (!g->sph_gauss_features || !g->bandwidth_sharpness || !g->lobe_axis))

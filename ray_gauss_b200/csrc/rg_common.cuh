@@ -144,10 +144,16 @@ struct __align__(16) GaussRec {
 // Wide traversal nodes.  Every binary node at a depth that is a multiple of kWideLevels owns the
 // frontier of its subtree kWideLevels levels down (binary nodes there, or leaves reached earlier):
 // at most kWideSlots children, stored as consecutive slots in leaf order.  A slot holds the child's
-// box, its id (>= 0 the binary index of a wide node, < 0 leaf ~index) and the last leaf of its
-// subtree (the multi-pass cursor test).  32 bytes, read with one 256-bit load per lane.
+// box, its id and the last leaf of its subtree (the multi-pass cursor test).  The id of a leaf
+// child is ~leaf (< 0); that of a wide child holds the child's own slots, first slot | (count - 1)
+// << kWideCountShift (>= 0), so a visit needs no other load.  32 bytes, one 256-bit load per lane.
 constexpr int kWideLevels = 5;
 constexpr int kWideSlots = 1 << kWideLevels;
+constexpr int kWideCountShift = 26;                       // first slot < 2^26: at most 2^25 Gaussians
+constexpr long long kMaxGaussians = 1ll << 25;
+__host__ __device__ __forceinline__ int wide_pack(int first, int count) {
+    return first | ((count - 1) << kWideCountShift);
+}
 struct __align__(32) WideSlot {
     float lo[3], hi[3];
     int id;

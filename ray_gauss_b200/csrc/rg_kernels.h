@@ -36,7 +36,7 @@ struct RenderArgs {
     const LeafIS* is_rec;
     const float4* ext;
     const float4* rgb;            // (n_views, n_leaves) leaf order
-    const int2* wide_tab;         // wide node of binary node i: {first slot, slot count}
+    const int2* wide_tab;         // wide node of binary node i: {first slot, slot count} (root: entry 0)
     const WideSlot* slots;        // wide-node children
     int n_leaves;
     const int* scene_ord;

@@ -14,8 +14,9 @@
 // counter).  Each lane marches its own ray with the reference's slab sequence (tb += 0.02 in
 // FP32); the warp advances in chunks of K slabs per lane (K adapts between 1 and 255: it grows
 // while hits are sparse and halves when the hit list overflows).  For a chunk the warp traverses
-// the wide BVH once for the beam of its lanes' segments (one child slot per lane against the
-// beam's planes) with a warp-uniform stack, runs the exact ellipsoid test per lane at the leaves
+// the wide BVH once for the packet of its lanes' segments (one child slot per lane, tested with
+// interval arithmetic over the lanes' directions) with a warp-uniform stack, runs the exact
+// ellipsoid test per lane at the leaves
 // and appends every leaf that any lane hits to a shared hit
 // list with, per lane, the range of the chunk's slabs its interval covers (exact for K <= 8; one
 // slab of margin on each side for longer chunks, where the extra slabs' samples fall outside the
@@ -55,8 +56,6 @@ constexpr int kCounters = 9;
 constexpr unsigned kNoRecord = 0xffffffffu;     // hit-list record: no (next) chunk record
 constexpr unsigned kRecordMulti = 0x80000000u;  // chunk consumed in several traversal passes
 constexpr unsigned kRecordFailed = 0xfffffffeu; // the tile's record did not fit the arena
-constexpr int kFrustumPlanes = 6;               // 4 sides through the eye, near and far along the axis
-constexpr int kFrustumFloats = 8 * kFrustumPlanes;
 
 // Warp hit-list layout.  Parity arithmetic keeps, per entry and lane, the exact range of the
 // chunk's slabs the lane's interval covers (64 B per entry); the fast arithmetic keeps only the mask
@@ -75,7 +74,7 @@ struct WarpSmem {
     unsigned short lrng[FAST ? 1 : CAP][32];         // parity: per lane lo | hi << 8 (lo > hi: no hit)
     unsigned smask[NB][CAP / 32];                    // entries whose union range meets block k / MB
     unsigned long long occ[4];                       // slabs holding any entry (union occupancy)
-    __align__(16) float frustum[kFrustumFloats];     // the chunk's beam: cull planes, read as float4
+    __align__(16) float packet[24];                  // the chunk's ray packet (set_packet), read as float4
     int stack[kStack];
     // hit-list record of the warp's current tile (written by lane 0)
     unsigned rec_first, rec_prev;                    // forward: first / last chunk record
@@ -123,91 +122,79 @@ __device__ __forceinline__ void load_slot(const WideSlot* p, float3& lo, float3&
     range_hi = u[1];
 }
 
-// Beam of a warp's chunk: the rays through the sample positions of the active lanes' pixel
-// rectangle (pixel centres; with jitter the [x + 1/3, x + 2/3) range the jittered samples take)
-// between the nearest start and the farthest end of the active lanes' chunk segments, measured
-// along the tile's central axis.  Six planes, each stored as the positive and
-// negative parts of its normal and an offset: a box lies outside when the largest value of n . x
-// over the box is below the offset.  The planes are widened by a slack far above the rounding of
-// the plane and box arithmetic, so the beam contains every ray segment the lanes test: the exact
-// per-lane leaf test decides the hits, the beam only skips subtrees no active ray can reach.
-__device__ __forceinline__ void set_plane(float* F, int i, float3 n, float off) {
-    F[8 * i + 0] = fmaxf(n.x, 0.f);
-    F[8 * i + 1] = fmaxf(n.y, 0.f);
-    F[8 * i + 2] = fmaxf(n.z, 0.f);
-    F[8 * i + 3] = fminf(n.x, 0.f);
-    F[8 * i + 4] = fminf(n.y, 0.f);
-    F[8 * i + 5] = fminf(n.z, 0.f);
-    F[8 * i + 6] = off;
-    F[8 * i + 7] = 0.f;
-}
-__device__ __forceinline__ float3 cross3(float3 a, float3 b) {
-    return f3(a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x);
-}
-// Unnormalised direction of the camera ray through image coordinates (u, v) in [0, 1]^2 (the ray
-// generation's d before normalisation, linear in u and v).
-__device__ __forceinline__ float3 pixel_dir(const rg_camera& cam, float u, float v) {
-    const float dx = (2.f * u - 1.f) * cam.tan_half_fovx, dy = (2.f * v - 1.f) * cam.tan_half_fovy;
-    return f3(cam.u[0] * dx + cam.v[0] * dy + cam.w[0], cam.u[1] * dx + cam.v[1] * dy + cam.w[1],
-              cam.u[2] * dx + cam.v[2] * dy + cam.w[2]);
-}
-
+// The chunk's ray packet for the wide-node test (interval arithmetic).  All rays start at the eye;
+// over the active lanes, per axis the direction component lies in [dmin, dmax] and the ray
+// parameter of the chunk segments in [tmin, tmax].  For a box, a ray's entry and exit parameters
+// along axis a are the smaller and larger of (lo_a - o_a) / d_a and (hi_a - o_a) / d_a, linear in
+// 1 / d_a: over the packet they lie between the products at the ends of the 1 / d interval, so the
+// box can meet a segment only if the largest of the smallest entries (and tmin) does not exceed
+// the smallest of the largest exits (and tmax).  Exact for one ray, conservative for a packet, tight
+// for the nearly parallel rays of a tile.  An axis whose direction interval holds 0 gives no bound
+// there; the box of the packet's segments (o + t d over the t and d intervals) bounds every axis.
+// Stored per axis {1/dmax, 1/dmin, -o/dmax, -o/dmin}, then {tmin - slack, tmax + slack}, then the
+// segments' box {lo.xyz, -}, {hi.xyz, -} widened by a position slack.  The
+// products round like the per-ray slab test's t = b/d - o/d: a few ulps of |o| in position, far
+// inside the leaf boxes' 1e-5 inflation, so the bound needs no slack of its own; a small one in t
+// covers the ends of the segments.  (A slack that grows with 1/|d| would stretch the packets of
+// rays nearly parallel to a coordinate plane over most of their length.)
 template <bool FAST, int CAP>
-__device__ __forceinline__ void set_frustum(WarpSmem<FAST, CAP>& sm, const rg_camera& cam, int jitter, int px,
-                                            int py, const RayState& r, bool on, float seg_hi, int lane) {
-    const unsigned x0 = __reduce_min_sync(kFull, on ? (unsigned)px : 0x7fffffffu);
-    const unsigned x1 = __reduce_max_sync(kFull, on ? (unsigned)px : 0u);
-    const unsigned y0 = __reduce_min_sync(kFull, on ? (unsigned)py : 0x7fffffffu);
-    const unsigned y1 = __reduce_max_sync(kFull, on ? (unsigned)py : 0u);
-    // the active segments along the axis (t along a unit ray direction d is t (ax . d) along the axis)
-    const float iW = 1.f / (float)cam.width, iH = 1.f / (float)cam.height;
-    const float lo = jitter == 1 ? 0.333333f : 0.5f, hi = jitter == 1 ? 0.666667f : 0.5f;
-    const float u0 = ((float)x0 + lo) * iW, u1 = ((float)x1 + hi) * iW;
-    const float v0 = ((float)y0 + lo) * iH, v1 = ((float)y1 + hi) * iH;
-    const float3 dc = pixel_dir(cam, 0.5f * (u0 + u1), 0.5f * (v0 + v1));
-    const float3 ax = dc * rsqrtf(dot3(dc, dc));
-    const float cd = dot3(ax, r.d);
-    const float s0 = fmaxf(r.tb * cd, 0.f), s1 = fmaxf(seg_hi * cd, 0.f);
-    const float s_near = __uint_as_float(__reduce_min_sync(kFull, on ? __float_as_uint(s0) : 0x7f800000u));
-    const float s_far = __uint_as_float(__reduce_max_sync(kFull, on ? __float_as_uint(s1) : 0u));
-    if (lane == 0) {
-        const float3 eye = f3(cam.eye[0], cam.eye[1], cam.eye[2]);
-        const float3 U = f3(cam.u[0], cam.u[1], cam.u[2]), V = f3(cam.v[0], cam.v[1], cam.v[2]);
-        const float ae = dot3(ax, eye);
-        const float slack = 2e-5f * (s_far + fabsf(eye.x) + fabsf(eye.y) + fabsf(eye.z) + 1.f);
-        // Side planes through the eye: the rays along a row of sample positions span the camera's
-        // U axis and the row's corner ray, the rays along a column span V and the column's corner
-        // ray, so each side plane holds one camera axis and one corner ray (well conditioned for
-        // any rectangle, a single pixel included).  Inside: towards larger v below the top edge,
-        // smaller v above the bottom edge, and likewise in u.
-        const float3 axis[4] = {U, U, V, V};
-        const float3 corner[4] = {pixel_dir(cam, u0, v0), pixel_dir(cam, u0, v1), pixel_dir(cam, u0, v0),
-                                  pixel_dir(cam, u1, v0)};
-        const float3 toward[4] = {V, V * -1.f, U, U * -1.f};
+__device__ __forceinline__ void set_packet(WarpSmem<FAST, CAP>& sm, const RayState& r, bool on, float seg_hi,
+                                           int lane) {
+    float dmin[3], dmax[3];
+    const float dv[3] = {r.d.x, r.d.y, r.d.z};
 #pragma unroll
-        for (int i = 0; i < 4; ++i) {
-            float3 n = cross3(axis[i], corner[i]);
-            if (dot3(n, toward[i]) < 0.f) n = n * -1.f;
-            n = n * rsqrtf(fmaxf(dot3(n, n), 1e-30f));
-            set_plane(sm.frustum, i, n, dot3(n, eye) - slack);
+    for (int a = 0; a < 3; ++a) {
+        dmin[a] = ord2f(__reduce_min_sync(kFull, on ? f2ord(dv[a]) : 0x7fffffff));
+        dmax[a] = ord2f(__reduce_max_sync(kFull, on ? f2ord(dv[a]) : (int)0x80000000));
+    }
+    const float tmin = __uint_as_float(__reduce_min_sync(kFull, on ? __float_as_uint(fmaxf(r.tb, 0.f)) : 0x7f800000u));
+    const float tmax = __uint_as_float(__reduce_max_sync(kFull, on ? __float_as_uint(fmaxf(seg_hi, 0.f)) : 0u));
+    if (lane == 0) {
+        const float ov[3] = {r.o.x, r.o.y, r.o.z};
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+            float4 q;
+            if (!(dmin[a] > 0.f) && !(dmax[a] < 0.f)) {
+                q = make_float4(0.f, 0.f, -INFINITY, INFINITY);   // the interval holds 0: no bound
+            } else {
+                const float rA = 1.f / dmax[a], rB = 1.f / dmin[a];
+                q = make_float4(rA, rB, -ov[a] * rA, -ov[a] * rB);
+            }
+            *reinterpret_cast<float4*>(sm.packet + 4 * a) = q;
         }
-        set_plane(sm.frustum, 4, ax, ae + s_near - slack);
-        set_plane(sm.frustum, 5, ax * -1.f, -(ae + s_far) - slack);
+        const float slack = 1e-6f * (tmax + 1.f);
+        *reinterpret_cast<float4*>(sm.packet + 12) = make_float4(tmin - slack, tmax + slack, 0.f, 0.f);
+        const float pslack = 1e-6f * (fabsf(ov[0]) + fabsf(ov[1]) + fabsf(ov[2]) + tmax + 1.f);
+        float bl[3], bh[3];
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+            const float e0 = tmin * dmin[a], e1 = tmin * dmax[a], e2 = tmax * dmin[a], e3 = tmax * dmax[a];
+            bl[a] = ov[a] + fminf(fminf(e0, e1), fminf(e2, e3)) - pslack;
+            bh[a] = ov[a] + fmaxf(fmaxf(e0, e1), fmaxf(e2, e3)) + pslack;
+        }
+        *reinterpret_cast<float4*>(sm.packet + 16) = make_float4(bl[0], bl[1], bl[2], 0.f);
+        *reinterpret_cast<float4*>(sm.packet + 20) = make_float4(bh[0], bh[1], bh[2], 0.f);
     }
     __syncwarp();
 }
 
-// Whether a box meets the beam: for every plane the largest n . x over the box reaches its offset.
-__device__ __forceinline__ bool beam_hit(const float* F, float3 lo, float3 hi) {
-    bool in = true;
-#pragma unroll
-    for (int i = 0; i < kFrustumPlanes; ++i) {
-        const float4 a = *reinterpret_cast<const float4*>(F + 8 * i);
-        const float4 b = *reinterpret_cast<const float4*>(F + 8 * i + 4);
-        const float m = fmaf(a.x, hi.x, fmaf(a.y, hi.y, fmaf(a.z, hi.z, fmaf(a.w, lo.x, fmaf(b.x, lo.y, b.y * lo.z)))));
-        in = in && (m >= b.z);
-    }
-    return in;
+__device__ __forceinline__ void packet_axis(float4 q, float lo, float hi, float& tin, float& tout) {
+    const float p1 = fmaf(lo, q.x, q.z), p2 = fmaf(lo, q.y, q.w), p3 = fmaf(hi, q.x, q.z), p4 = fmaf(hi, q.y, q.w);
+    tin = fminf(fminf(p1, p2), fminf(p3, p4));
+    tout = fmaxf(fmaxf(p1, p2), fmaxf(p3, p4));
+}
+
+// Whether a box may meet a segment of the packet (see set_packet).
+__device__ __forceinline__ bool packet_hit(const float* F, float3 lo, float3 hi) {
+    const float4 qx = *reinterpret_cast<const float4*>(F), qy = *reinterpret_cast<const float4*>(F + 4),
+                 qz = *reinterpret_cast<const float4*>(F + 8), qt = *reinterpret_cast<const float4*>(F + 12);
+    const float4 bl = *reinterpret_cast<const float4*>(F + 16), bh = *reinterpret_cast<const float4*>(F + 20);
+    float ix, ox, iy, oy, iz, oz;
+    packet_axis(qx, lo.x, hi.x, ix, ox);
+    packet_axis(qy, lo.y, hi.y, iy, oy);
+    packet_axis(qz, lo.z, hi.z, iz, oz);
+    const bool in_box = lo.x <= bh.x && hi.x >= bl.x && lo.y <= bh.y && hi.y >= bl.y && lo.z <= bh.z && hi.z >= bl.z;
+    return in_box && fmaxf(max3f(ix, iy, iz), qt.x) <= fminf(min3f(ox, oy, oz), qt.y);
 }
 
 __device__ __forceinline__ LeafRec load_rec(const LeafRec* p, int i) {
@@ -476,8 +463,8 @@ __device__ __forceinline__ void finish_list(WarpSmem<FAST, CAP>& sm, int count, 
     __syncwarp();
 }
 
-// Warp-cooperative traversal for the chunk [tb, seg_hi] of every active lane (the beam set by
-// set_frustum).  At a wide node lane k tests child slot k against the beam; the first hit child is
+// Warp-cooperative traversal for the chunk [tb, seg_hi] of every active lane (the packet set by
+// set_packet).  At a wide node lane k tests child slot k against the packet; the first hit child is
 // visited next and the others wait on the stack, the lowest index on top, so leaves are reached in
 // increasing index (the multi-pass cursor relies on it).  Appends hit leaves with index > cursor to
 // the warp list; returns the entry count.  `ovf` is set when the list filled up before the
@@ -490,7 +477,11 @@ __device__ int traverse(WarpSmem<FAST, CAP>& sm, const RenderArgs& a, const RayS
     ovf = false;
     clear_occ(sm, lane);
     int sp = 0;
-    int cur = (a.n_leaves == 1) ? ~0 : 0;
+    int cur = ~0;   // one Gaussian: the root is a leaf
+    if (a.n_leaves > 1) {
+        const int2 root = __ldg(a.wide_tab);
+        cur = wide_pack(root.x, root.y);
+    }
     unsigned guard = 0, visits = 0;
     const unsigned guard_max = 2u * (unsigned)a.n_leaves + 64u;
     while (true) {
@@ -500,14 +491,14 @@ __device__ int traverse(WarpSmem<FAST, CAP>& sm, const RenderArgs& a, const RayS
         }
         if (cur >= 0) {
             if (DIAG) ++visits;
-            const int2 wt = __ldg(a.wide_tab + cur);
+            const int first = cur & ((1 << kWideCountShift) - 1), count = (cur >> kWideCountShift) + 1;
             bool hit = false;
             int cid = 0;
-            if (lane < wt.y) {
+            if (lane < count) {
                 float3 lo, hi;
                 int range_hi;
-                load_slot(a.slots + wt.x + lane, lo, hi, cid, range_hi);
-                hit = (range_hi > cursor) && beam_hit(sm.frustum, lo, hi);
+                load_slot(a.slots + first + lane, lo, hi, cid, range_hi);
+                hit = (range_hi > cursor) && packet_hit(sm.packet, lo, hi);
             }
             const unsigned hm = __ballot_sync(kFull, hit);
             if (hm) {
@@ -576,29 +567,47 @@ __device__ __forceinline__ unsigned slab_offsets(int rnd_sample, unsigned seed, 
     return seed;
 }
 
-// Reference-order evaluation of one sample's weight with an exact threshold decision.
-__device__ __forceinline__ float parity_weight(float3 o, float3 d, float t, float3 mu, float3 r0, float3 r1,
-                                               float3 r2, float dn, float3& v, float3& m, bool& in) {
-    float3 x = f3(__fadd_rn(o.x, __fmul_rn(d.x, t)), __fadd_rn(o.y, __fmul_rn(d.y, t)),
-                  __fadd_rn(o.z, __fmul_rn(d.z, t)));
-    v = f3(__fsub_rn(x.x, mu.x), __fsub_rn(x.y, mu.y), __fsub_rn(x.z, mu.z));
-    m = rows_rn(r0, r1, r2, v);
-    float power = __fmul_rn(-0.5f, dot_rn(m, m));
-    float w = expf(power);
-    float dw = __fmul_rn(dn, w);
-    if (fabsf(dw - kSigThr) < 4e-8f) {
-        // within the exponential's error of the threshold: decide with a correctly rounded weight
-        w = (float)exp((double)power);
-        dw = __fmul_rn(dn, w);
-    }
-    in = dw > kSigThr;
-    return w;
+// Exponent -|M (o + t d - mu)|^2 / 2 of a sample in the reference's operation order.
+__device__ __forceinline__ float parity_power(float3 o, float3 d, float t, float3 mu, float3 r0, float3 r1,
+                                              float3 r2) {
+    const float3 x = f3(__fadd_rn(o.x, __fmul_rn(d.x, t)), __fadd_rn(o.y, __fmul_rn(d.y, t)),
+                        __fadd_rn(o.z, __fmul_rn(d.z, t)));
+    const float3 v = f3(__fsub_rn(x.x, mu.x), __fsub_rn(x.y, mu.y), __fsub_rn(x.z, mu.z));
+    const float3 m = rows_rn(r0, r1, r2, v);
+    return __fmul_rn(-0.5f, dot_rn(m, m));
 }
 
 __device__ __forceinline__ float parity_time(float tb, int i, int rnd_sample, const float* roff) {
     float t = __fadd_rn(tb, __fmul_rn((float)i, kDt));
     if (rnd_sample) t = __fadd_rn(t, roff[i]);
     return t;
+}
+
+// Reference-order weights w[i] of the 8 samples of a slab for one Gaussian, and the mask of the
+// samples whose density * weight exceeds 0.1.  The eight weights are computed first, without
+// branches, so their dependency chains interleave; a sample whose density * weight lies within the
+// exponential's error of 0.1 is then re-evaluated with a correctly rounded weight, so that the
+// threshold decision is the one of the FP32 reference arithmetic.
+__device__ __forceinline__ unsigned parity_weights(const RayState& r, int rnd_sample, const float* roff, float3 mu,
+                                                   float3 r0, float3 r1, float3 r2, float dn, float* w) {
+    unsigned near = 0u;
+#pragma unroll
+    for (int i = 0; i < kBuf; ++i) {
+        w[i] = expf(parity_power(r.o, r.d, parity_time(r.tb, i, rnd_sample, roff), mu, r0, r1, r2));
+        near |= (fabsf(__fmul_rn(dn, w[i]) - kSigThr) < 4e-8f ? 1u : 0u) << i;
+    }
+    if (near) {
+#pragma unroll
+        for (int i = 0; i < kBuf; ++i) {
+            if ((near >> i) & 1u)
+                w[i] = (float)exp((double)parity_power(r.o, r.d, parity_time(r.tb, i, rnd_sample, roff), mu, r0, r1,
+                                                       r2));
+        }
+    }
+    unsigned in = 0u;
+#pragma unroll
+    for (int i = 0; i < kBuf; ++i) in |= (__fmul_rn(dn, w[i]) > kSigThr ? 1u : 0u) << i;
+    return in;
 }
 
 __device__ __forceinline__ bool in_range(unsigned short rg, int k) {
@@ -694,13 +703,12 @@ __device__ __forceinline__ int slab_buffers(const WarpSmem<FAST, CAP>& sm, int k
                     m = f3(__fadd_rn(m.x, mdt.x), __fadd_rn(m.y, mdt.y), __fadd_rn(m.z, mdt.z));
                 }
             } else {
+                float ws[kBuf];
+                const unsigned in_mask = parity_weights(r, a.rnd_sample, roff, mu, r0, r1, r2, dn, ws);
 #pragma unroll
                 for (int i = 0; i < kBuf; ++i) {
-                    float t = parity_time(r.tb, i, a.rnd_sample, roff);
-                    float3 v, m;
-                    bool in;
-                    float w = parity_weight(r.o, r.d, t, mu, r0, r1, r2, dn, v, m, in);
-                    if (in) {
+                    const float w = ws[i];
+                    if ((in_mask >> i) & 1u) {
                         sig[i] = __fadd_rn(sig[i], __fmul_rn(dn, w));
                         if (GDOT) {
                             gC[i] += (r.g.x * col4.x + r.g.y * col4.y + r.g.z * col4.z) * (w * dn);
@@ -867,13 +875,13 @@ __device__ __forceinline__ void slab_adjoint(const WarpSmem<FAST, CAP>& sm, int 
                 }
                 dd = (U0 != 0.f) ? U0 * rec.r2.w : 0.f;                   // r2.w = 1 / dens
             } else {
+                float ws[kBuf];
+                const unsigned in_mask = parity_weights(r, a.rnd_sample, roff, mu, r0, r1, r2, dn, ws);
 #pragma unroll
                 for (int i = 0; i < kBuf; ++i) {
-                    float t = parity_time(r.tb, i, a.rnd_sample, roff);
-                    float3 vv, m;
-                    bool in;
-                    float wt = parity_weight(r.o, r.d, t, mu, r0, r1, r2, dn, vv, m, in);
-                    if (in) {
+                    if ((in_mask >> i) & 1u) {
+                        const float wt = ws[i];
+                        const float t = parity_time(r.tb, i, a.rnd_sample, roff);
                         float h = fmaf(F[i], gcol, H[i]);
                         gc += wt * F[i];
                         dd += wt * h;
@@ -1109,7 +1117,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, min_blocks<BWD, FAST>()) 
             bool ovf = false;
             int count;
             const bool replayed = BWD && rec_cur != kNoRecord && !(rec_hdr & kRecordMulti);
-            if (!replayed) set_frustum<FAST, CAP>(sm, a.cams[view], a.jitter, px, py, r, on, seg_hi, lane);
+            if (!replayed) set_packet<FAST, CAP>(sm, r, on, seg_hi, lane);
             if (replayed) {
                 const unsigned n_ids = min(rec_hdr & 0xffffu, a.rec_cap - rec_cur - 2u);
                 count = replay_list<FAST, CAP, DIAG>(sm, a, r, on, seg_hi, K, nv, a.rec_arena + rec_cur + 2, (int)n_ids,
@@ -1339,13 +1347,13 @@ size_t render_smem_bytes(bool, int cap) {
     return sizeof(WarpSmem<false, 128>) * kWarpsPerBlock;
 }
 static_assert(sizeof(WarpSmem<false, 128>) * kWarpsPerBlock <= 48 * 1024, "static shared memory limit");
-// the beam planes are read as float4: 16-byte aligned in every warp's slice of the block's array
+// the packet is read as float4: 16-byte aligned in every warp's slice of the block's array
 using ParitySmem = WarpSmem<false, 128>;
 using FastSmem256 = WarpSmem<true, 256>;
 using FastSmem512 = WarpSmem<true, 512>;
-static_assert(offsetof(ParitySmem, frustum) % 16 == 0 && sizeof(ParitySmem) % 16 == 0, "beam plane alignment");
-static_assert(offsetof(FastSmem256, frustum) % 16 == 0 && sizeof(FastSmem256) % 16 == 0, "beam plane alignment");
-static_assert(offsetof(FastSmem512, frustum) % 16 == 0 && sizeof(FastSmem512) % 16 == 0, "beam plane alignment");
+static_assert(offsetof(ParitySmem, packet) % 16 == 0 && sizeof(ParitySmem) % 16 == 0, "packet alignment");
+static_assert(offsetof(FastSmem256, packet) % 16 == 0 && sizeof(FastSmem256) % 16 == 0, "packet alignment");
+static_assert(offsetof(FastSmem512, packet) % 16 == 0 && sizeof(FastSmem512) % 16 == 0, "packet alignment");
 static_assert(sizeof(WarpSmem<true, 512>) * kWarpsPerBlock <= 48 * 1024, "static shared memory limit");
 
 template <bool BWD, bool FAST>
