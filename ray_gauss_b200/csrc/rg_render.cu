@@ -970,10 +970,10 @@ __device__ __forceinline__ void slab_adjoint_scalars(const RayState& r, const fl
 #define RG_FAST_BWD_MIN_BLOCKS 7
 #endif
 #ifndef RG_PAR_FWD_MIN_BLOCKS
-#define RG_PAR_FWD_MIN_BLOCKS 5
+#define RG_PAR_FWD_MIN_BLOCKS 4
 #endif
 #ifndef RG_PAR_BWD_MIN_BLOCKS
-#define RG_PAR_BWD_MIN_BLOCKS 5
+#define RG_PAR_BWD_MIN_BLOCKS 4
 #endif
 template <bool BWD, bool FAST>
 constexpr int min_blocks() {
