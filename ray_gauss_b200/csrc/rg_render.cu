@@ -51,7 +51,7 @@ constexpr float kInvSlab = 50.0f;          // 1 / 0.02
 constexpr int kExactChunk = 8;             // chunks up to this length use exact slab ranges
 constexpr int kCounters = 9;
 #ifndef RG_DIRECT_ATOMIC_LANES
-#define RG_DIRECT_ATOMIC_LANES 16  // up to this many contributing lanes add with float4 atomics directly
+#define RG_DIRECT_ATOMIC_LANES 24  // up to this many contributing lanes add with float4 atomics directly
 #endif               // per-warp counters: the WarpStats fields, hit pairs, slabs
 constexpr unsigned kNoRecord = 0xffffffffu;     // hit-list record: no (next) chunk record
 constexpr unsigned kRecordMulti = 0x80000000u;  // chunk consumed in several traversal passes
