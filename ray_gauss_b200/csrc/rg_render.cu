@@ -239,16 +239,18 @@ __device__ __forceinline__ bool roots_fast(const LeafRec& rec, const RayState& r
            r2 = f3(rec.r2.x, rec.r2.y, rec.r2.z);
     float3 Oe = f3(dot3(r0, O) * k, dot3(r1, O) * k, dot3(r2, O) * k);
     float3 De = f3(dot3(r0, r.d) * k, dot3(r1, r.d) * k, dot3(r2, r.d) * k);
-    float l = 1.f / sqrtf(dot3(De, De));
+    // SFU reciprocal square roots and a fast division (the fast arithmetic's interval ends move by
+    // ulps; the forward and the backward's replay run this same test)
+    float l = rsqrtf(dot3(De, De));
     float3 Dn = De * l;
     float b = -dot3(Oe, Dn);
     float c = dot3(Oe, Oe) - 1.f;
     float3 p = Oe + Dn * b;
     float disc = 1.f - dot3(p, p);
     if (!(disc > 1e-7f)) return false;
-    float sd = sqrtf(disc);
-    float q = b + (b > 0.f ? sd : -sd);
-    root1 = (c / q) * l;
+    float sd = disc * rsqrtf(disc);
+    float q = b + (b > 0.f ? sd : -sd);   // |q| >= sd > 3e-4
+    root1 = __fdividef(c, q) * l;
     root2 = q * l;
     return true;
 }
