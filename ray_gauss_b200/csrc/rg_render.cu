@@ -744,6 +744,12 @@ __device__ __forceinline__ bool any_density(const float* sig) {
 template <bool FAST>
 __device__ __forceinline__ void composite(RayState& r, const float* sig, const float3* C) {
     if (!any_density(sig)) return;
+    float ex[kBuf];
+    if (!FAST) {
+        // the eight exponentials are independent of the transmittance chain: evaluate them first
+#pragma unroll
+        for (int i = 0; i < kBuf; ++i) ex[i] = exp_neg<false>(__fmul_rn(sig[i], kDt));
+    }
 #pragma unroll
     for (int i = 0; i < kBuf; ++i) {
         if (FAST) {
@@ -753,7 +759,7 @@ __device__ __forceinline__ void composite(RayState& r, const float* sig, const f
             r.C = r.C + C[i] * s;
             r.T *= 1.f - alpha;
         } else {
-            float alpha = __fsub_rn(1.f, exp_neg<false>(__fmul_rn(sig[i], kDt)));
+            float alpha = __fsub_rn(1.f, ex[i]);
             float3 c = C[i];
             if (sig[i] > 0.f) {
                 float inv = __fdiv_rn(1.f, sig[i]);
@@ -947,13 +953,18 @@ __device__ __forceinline__ void slab_adjoint_scalars(const RayState& r, const fl
                                                      float* F, float& Ta, float& gRa) {
     Ta = r.T;
     gRa = r.gR;
+    float ex[kBuf];
+    if (!FAST) {
+#pragma unroll
+        for (int i = 0; i < kBuf; ++i) ex[i] = exp_neg<false>(__fmul_rn(sig[i], kDt));
+    }
 #pragma unroll
     for (int i = 0; i < kBuf; ++i) {
         const float cd = sig[i];
         float inv = 0.f;
         if (cd > 0.f) inv = FAST ? __fdividef(1.f, cd) : 1.f / cd;
         const float gc = gC[i] * inv;
-        const float alpha = FAST ? 1.f - exp_neg<true>(cd * kDt) : __fsub_rn(1.f, exp_neg<false>(__fmul_rn(cd, kDt)));
+        const float alpha = FAST ? 1.f - exp_neg<true>(cd * kDt) : __fsub_rn(1.f, ex[i]);
         const float ta = Ta * alpha;
         F[i] = ta * inv;
         H[i] = kDt * (Ta * gc - gRa) - F[i] * gc;
