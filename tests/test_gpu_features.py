@@ -188,3 +188,20 @@ def test_graphed_step_with_the_reference_loss(cuda):
     for k in KEYS:
         if Q[k].grad is not None and Q[k].numel():
             assert rel_l2(step.grads[k].cpu().numpy(), Q[k].grad.cpu().numpy()) <= 1e-4, k
+
+
+def test_engine_rejects_more_gaussians_than_wide_node_ids_address(cuda):
+    """Wide-node child ids pack the first slot and the child count into 32 bits, which addresses
+    2^25 Gaussians: a larger cloud is refused on the host (RG_ERR_INVALID_ARG) before any device
+    work, and the engine stays usable."""
+    import ctypes
+    from ray_gauss_b200.engine import Engine, make_gaussians
+    P, _ = _scene(cuda, n=500)
+    eng = Engine(cuda.index or 0)
+    g = make_gaussians(*(P[k] for k in KEYS))
+    g.struct.n = (1 << 25) + 1
+    rc = eng.lib.rg_ellipsoids_bbox(eng.h, ctypes.byref(g.struct), None, None, None)
+    assert rc == 1   # RG_ERR_INVALID_ARG
+    g.struct.n = 500
+    assert eng.lib.rg_ellipsoids_bbox(eng.h, ctypes.byref(g.struct), None, None, None) == 0
+    torch.cuda.synchronize()
