@@ -246,7 +246,7 @@ RG_API int rg_leaf_order(rg_engine* e, int32_t* leaf_gid_out, void* stream);
  * capture, fixed device-memory budgets, plugins that must not touch the process allocator).  No
  * counterpart in the reference.  Same pre-pass, LBVH build, colour pass and forward launch as
  * rg_render_forward (default tuning), without an engine: all scratch lives in one static device
- * array of about 11 MB that every GPU loading this library keeps until exit.  At most 16384
+ * array of about 10 MB that every GPU loading this library keeps until exit.  At most 16384
  * Gaussians and 4 views per call (RG_ERR_CAPACITY beyond).  Calls share that array, so calls that
  * overlap on the GPU race; the first call on a device resolves the array's address and should
  * come before any stream capture.  cams, ray_colors and final_T are device pointers as in

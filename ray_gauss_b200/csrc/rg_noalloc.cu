@@ -5,7 +5,7 @@
 // or plugins loaded into a process whose allocator must not be touched.  This entry point runs
 // the same pre-pass, LBVH build, colour pass and forward launch as rg_render_forward without an
 // engine and without allocating: all of its scratch lives in one file-scope device array of
-// kNoAllocScratchBytes (about 11 MB), which every GPU that loads this library holds until the
+// kNoAllocScratchBytes (about 10 MB), which every GPU that loads this library holds until the
 // process exits.  The caller still passes the Gaussians, cameras and output buffers.
 //
 // Limits: at most kNoAllocMaxGaussians (16384) Gaussians and kNoAllocMaxViews (4) views per call;
