@@ -21,7 +21,7 @@ struct rg_engine {
     rg::BvhBuffers bvh;
     float4* rgb_leaf = nullptr;      // (views, N)
     float4* gacc_geo = nullptr;      // (N, 3)
-    float4* gacc_rgb = nullptr;      // (views, N)
+    float4* gacc_rgb = nullptr;      // (N, views)
     rg::ViewTable* vt = nullptr;
     int* work_counter = nullptr;
     rg::DevStatus* st = nullptr;
@@ -495,6 +495,7 @@ int rg_launch_backward(rg_engine* e, const rg_camera* cams, int32_t n_cams, cons
     a.dL = dloss_dray_colors;
     a.gacc_geo = e->gacc_geo;
     a.gacc_rgb = e->gacc_rgb;
+    a.n_views = n_cams;
     // Replay the last forward's hit lists when nothing changed the engine state since that forward
     // (bbox, BVH, colour and tuning calls invalidate the record) and this backward uses the same
     // camera table, view count and settings: the chunk sequence is then the forward's.

@@ -108,8 +108,9 @@ __global__ void __launch_bounds__(128) k_color_fwd(long long n, const float* __r
     }
 }
 
-// One thread per Gaussian: gather the leaf-ordered accumulators, run the SH/SG backward for every
-// view, add the view-direction term to the position gradient and write all outputs.
+// One thread per Gaussian: gather the leaf-ordered accumulators, run the SH backward for every view,
+// add its view-direction term to the position gradient and write the geometry, density and SH
+// gradients.  The spherical Gaussians follow in k_color_bwd_sg.
 __global__ void __launch_bounds__(128) k_color_bwd(long long n, const float* __restrict__ pos,
                                                    const void* __restrict__ sh, const void* __restrict__ sg,
                                                    const float* __restrict__ kappa, const float* __restrict__ axis,
@@ -142,15 +143,9 @@ __global__ void __launch_bounds__(128) k_color_bwd(long long n, const float* __r
     for (int c = 0; c < 3; ++c)
 #pragma unroll
         for (int k = 0; k < 16; ++k) dsh[c][k] = 0.f;
-    for (int l = 0; l < nsg; ++l) {
-        long long b = g * nsg + l;
-        for (int c = 0; c < 3; ++c) out.sph_gauss_features[(g * 3 + c) * nsg + l] = 0.f;
-        out.bandwidth_sharpness[b] = 0.f;
-        out.lobe_axis[3 * b] = 0.f; out.lobe_axis[3 * b + 1] = 0.f; out.lobe_axis[3 * b + 2] = 0.f;
-    }
     float px = pos[3 * g], py = pos[3 * g + 1], pz = pos[3 * g + 2];
     for (int v = 0; v < n_cams; ++v) {
-        float4 gr4 = gacc_rgb[(long long)v * n + leaf];
+        float4 gr4 = gacc_rgb[(long long)leaf * n_cams + v];
         float gr[3] = {gr4.x, gr4.y, gr4.z};
         if (gr[0] == 0.f && gr[1] == 0.f && gr[2] == 0.f) continue;
         float dx = px - cams[v].eye[0], dy = py - cams[v].eye[1], dz = pz - cams[v].eye[2];
@@ -199,25 +194,6 @@ __global__ void __launch_bounds__(128) k_color_bwd(long long n, const float* __r
                 if (k < nsh) { sx += bx[k] * coef[c][k]; sy += by[k] * coef[c][k]; sz += bz[k] * coef[c][k]; }
             ddir[0] += gr[c] * sx; ddir[1] += gr[c] * sy; ddir[2] += gr[c] * sz;
         }
-        for (int l = 0; l < nsg; ++l) {
-            long long b = g * nsg + l;
-            float ax = axis[3 * b], ay = axis[3 * b + 1], az = axis[3 * b + 2];
-            float kap = kappa[b];
-            float cosm1 = (x * ax + y * ay + z * az) - 1.f;
-            float wgt = expf(cosm1 * kap);
-            float dldw = 0.f;
-            for (int c = 0; c < 3; ++c) {
-                out.sph_gauss_features[(g * 3 + c) * nsg + l] += gr[c] * wgt;
-                dldw += gr[c] * load_param(sg, (g * 3 + c) * nsg + l, storage);
-            }
-            out.lobe_axis[3 * b] += dldw * kap * x * wgt;
-            out.lobe_axis[3 * b + 1] += dldw * kap * y * wgt;
-            out.lobe_axis[3 * b + 2] += dldw * kap * z * wgt;
-            out.bandwidth_sharpness[b] += dldw * cosm1 * wgt;
-            ddir[0] += dldw * kap * wgt * ax;
-            ddir[1] += dldw * kap * wgt * ay;
-            ddir[2] += dldw * kap * wgt * az;
-        }
         // d(v/|v|)/dv applied to dL/ddir
         float inv3 = inv * inv * inv;
         float dv[3] = {dx, dy, dz};
@@ -237,6 +213,66 @@ __global__ void __launch_bounds__(128) k_color_bwd(long long n, const float* __r
     out.positions[3 * g] = dpos[0];
     out.positions[3 * g + 1] = dpos[1];
     out.positions[3 * g + 2] = dpos[2];
+}
+
+// The spherical-Gaussian part of the colour backward (utils/sh_utils.cu:121-315), one thread per
+// Gaussian, lobes outer and views inner: a lobe's amplitude, sharpness and axis gradients stay in
+// registers across the views and are written once; its view-direction term is added to the
+// position gradient k_color_bwd wrote.
+__global__ void __launch_bounds__(128) k_color_bwd_sg(long long n, const float* __restrict__ pos,
+                                                      const void* __restrict__ sg, const float* __restrict__ kappa,
+                                                      const float* __restrict__ axis, int nsg, int storage,
+                                                      const rg_camera* __restrict__ cams, int n_cams,
+                                                      const int* __restrict__ rank,
+                                                      const float4* __restrict__ gacc_rgb, rg_gradients out) {
+    long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= n) return;
+    const int leaf = rank[g];
+    const float px = pos[3 * g], py = pos[3 * g + 1], pz = pos[3 * g + 2];
+    float dpos[3] = {0.f, 0.f, 0.f};
+    for (int l = 0; l < nsg; ++l) {
+        const long long b = g * nsg + l;
+        const float ax = axis[3 * b], ay = axis[3 * b + 1], az = axis[3 * b + 2];
+        const float kap = kappa[b];
+        float amp[3];
+#pragma unroll
+        for (int c = 0; c < 3; ++c) amp[c] = load_param(sg, (g * 3 + c) * nsg + l, storage);
+        float damp[3] = {0.f, 0.f, 0.f}, dax[3] = {0.f, 0.f, 0.f}, dkap = 0.f;
+        for (int v = 0; v < n_cams; ++v) {
+            const float4 gr4 = gacc_rgb[(long long)leaf * n_cams + v];
+            if (gr4.x == 0.f && gr4.y == 0.f && gr4.z == 0.f) continue;
+            const float dx = px - cams[v].eye[0], dy = py - cams[v].eye[1], dz = pz - cams[v].eye[2];
+            const float s2 = dx * dx + dy * dy + dz * dz;
+            const float inv = 1.f / sqrtf(s2);
+            const float x = dx * inv, y = dy * inv, z = dz * inv;
+            const float cosm1 = (x * ax + y * ay + z * az) - 1.f;
+            const float wgt = expf(cosm1 * kap);
+            const float dldw = gr4.x * amp[0] + gr4.y * amp[1] + gr4.z * amp[2];
+            damp[0] += gr4.x * wgt; damp[1] += gr4.y * wgt; damp[2] += gr4.z * wgt;
+            dax[0] += dldw * kap * x * wgt;
+            dax[1] += dldw * kap * y * wgt;
+            dax[2] += dldw * kap * z * wgt;
+            dkap += dldw * cosm1 * wgt;
+            // d(v/|v|)/dv applied to this lobe's dL/ddir
+            const float ddir[3] = {dldw * kap * wgt * ax, dldw * kap * wgt * ay, dldw * kap * wgt * az};
+            const float inv3 = inv * inv * inv;
+            const float dv[3] = {dx, dy, dz};
+#pragma unroll
+            for (int a = 0; a < 3; ++a) {
+                float acc = 0.f;
+#pragma unroll
+                for (int c = 0; c < 3; ++c) acc += ((a == c ? s2 : 0.f) - dv[a] * dv[c]) * ddir[c];
+                dpos[a] += acc * inv3;
+            }
+        }
+#pragma unroll
+        for (int c = 0; c < 3; ++c) out.sph_gauss_features[(g * 3 + c) * nsg + l] = damp[c];
+        out.bandwidth_sharpness[b] = dkap;
+        out.lobe_axis[3 * b] = dax[0]; out.lobe_axis[3 * b + 1] = dax[1]; out.lobe_axis[3 * b + 2] = dax[2];
+    }
+    out.positions[3 * g] += dpos[0];
+    out.positions[3 * g + 1] += dpos[1];
+    out.positions[3 * g + 2] += dpos[2];
 }
 
 cudaError_t launch_setup_views(const rg_camera* cams, int n_cams, ViewTable* vt, int* work_counter, cudaStream_t s) {
@@ -262,6 +298,13 @@ cudaError_t launch_color_backward(const rg_gaussians* g, const rg_camera* cams, 
     k_color_bwd<<<blocks, 128, 0, s>>>(n, g->positions, g->color_features, g->sph_gauss_features,
                                        g->bandwidth_sharpness, g->lobe_axis, g->sh_degree, g->num_sph_gauss,
                                        g->storage, cams, n_cams, rank, gacc_geo, gacc_rgb, sh_quirk, *out);
+    if (g->num_sph_gauss > 0) {
+        cudaError_t e = cudaGetLastError();
+        if (e != cudaSuccess) return e;
+        k_color_bwd_sg<<<blocks, 128, 0, s>>>(n, g->positions, g->sph_gauss_features, g->bandwidth_sharpness,
+                                              g->lobe_axis, g->num_sph_gauss, g->storage, cams, n_cams, rank,
+                                              gacc_rgb, *out);
+    }
     return cudaGetLastError();
 }
 

@@ -51,7 +51,8 @@ struct RenderArgs {
     const float* dL;
     float4* gacc_geo;             // (n_leaves, 3): ddens, dpos.xyz, dscale.xyz, dquat.xyzw, pad (the
                                   // render kernel accumulates moments there; launch_moment_grads converts)
-    float4* gacc_rgb;             // (n_views, n_leaves): {drgb.xyz, 0}
+    float4* gacc_rgb;             // (n_leaves, n_views): {drgb.xyz, 0}, a leaf's views contiguous
+    int n_views = 0;              // views of the launch (the gacc_rgb row length)
     int* work_counter;
     DevStatus* st;
     // hit-list record: the forward appends each warp chunk's leaf ids to the arena (chunk records

@@ -824,7 +824,7 @@ template <bool FAST, int CAP, bool DIAG>
 __device__ __forceinline__ void slab_adjoint(const WarpSmem<FAST, CAP>& sm, int k, int K, bool has, const RayState& r,
                                              const RenderArgs& a, int rgb_base, const float* roff,
                                              const float* H, const float* F, int nw, int lane,
-                                             WarpStats& ws) {
+                                             WarpStats& ws, int view) {
     const int vid = ((lane >> 4) & 1) * 8 + ((lane >> 3) & 1) * 4 + ((lane >> 2) & 1) * 2 + ((lane >> 1) & 1);
 #pragma unroll 1
     for (int w = 0; w < nw; ++w) {
@@ -917,7 +917,7 @@ __device__ __forceinline__ void slab_adjoint(const WarpSmem<FAST, CAP>& sm, int 
             v[11] = r.g.x * gc; v[12] = r.g.y * gc; v[13] = r.g.z * gc;
         }
         float* gg = reinterpret_cast<float*>(a.gacc_geo + 3 * (long long)leaf);
-        float* gr = reinterpret_cast<float*>(a.gacc_rgb + rgb_base + leaf);
+        float* gr = reinterpret_cast<float*>(a.gacc_rgb + (long long)leaf * a.n_views + view);
         // lanes whose samples all fell under the threshold contribute nothing
         const bool nz = act && (v[0] != 0.f || v[1] != 0.f || v[2] != 0.f || v[3] != 0.f || v[11] != 0.f ||
                                 v[12] != 0.f || v[13] != 0.f);
@@ -1213,7 +1213,8 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, min_blocks<BWD, FAST>()) 
                         float H[kBuf], F[kBuf], Ta, gRa;
                         slab_adjoint_scalars<FAST>(r, sig, gC, H, F, Ta, gRa);
                         bool act = has && nh > 0 && any_density(sig);
-                        slab_adjoint<FAST, CAP, DIAG>(sm, k, K, act, r, a, rgb_base, roff, H, F, nwords(count), lane, ws);
+                        slab_adjoint<FAST, CAP, DIAG>(sm, k, K, act, r, a, rgb_base, roff, H, F, nwords(count), lane, ws,
+                                                      view);
                         if (has && nh > 0) {
                             r.T = Ta;
                             r.gR = gRa;
@@ -1270,7 +1271,8 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, min_blocks<BWD, FAST>()) 
                     bool more2 = true;
                     while (more2) {
                         count = traverse<FAST, CAP, DIAG>(sm, a, r, on, seg_hi, 1, nv, cursor, more2, lane, ws, infer);
-                        slab_adjoint<FAST, CAP, DIAG>(sm, 0, 1, act, r, a, rgb_base, roff, H, F, nwords(count), lane, ws);
+                        slab_adjoint<FAST, CAP, DIAG>(sm, 0, 1, act, r, a, rgb_base, roff, H, F, nwords(count), lane, ws,
+                                                      view);
                         if (more2) cursor = sm.ids[count - 1];
                         __syncwarp();
                     }
