@@ -341,3 +341,30 @@ def test_fast_mode_bf16_storage_small_object_full_size(cuda, oracle):
     assert np.abs(img - ref_img).max() <= 5e-4
     for k, v in ref_g.items():
         assert rel_l2(g[k], v) <= GRAD_TOL, (k, rel_l2(g[k], v))
+
+
+def test_supersampling_is_the_finer_ray_grid(cuda):
+    """Supersampling (ssx, ssy) traces the image's W*ssx x H*ssy ray grid (optix_utils.py:132,
+    168-169; forward/gaussians_aabb.cu:405-434): the same camera at twice the width gives the same rays, so
+    the (2, 1)-supersampled render and its gradients equal that camera's, bit for bit."""
+    from ray_gauss_b200 import synthetic as S
+    from ray_gauss_b200.optix_raycasting.render_optix import RenderOptixFunction, RenderOptixSettings
+    p, _, white = S.workload("small_object", n=2000, seed=5)
+    P = {k: v.to(cuda).contiguous() for k, v in p.items()}
+    nsg = P["sph_gauss_features"].shape[2]
+    eye = [0.4, -2.6, 1.3]
+    cam_ss = S.look_at_camera(eye, [0.0, 0.0, 0.0], 24, 18, fovx=0.7, fovy=0.55, device=cuda)
+    cam_2w = S.look_at_camera(eye, [0.0, 0.0, 0.0], 48, 18, fovx=0.7, fovy=0.55, device=cuda)
+    dL = torch.randn((48 * 18, 3), device=cuda, generator=torch.Generator(device=cuda).manual_seed(2)) * 1e-2
+    outs = []
+    for cam, ss in ((cam_ss, (2, 1)), (cam_2w, (1, 1))):
+        Q = {k: v.detach().clone().requires_grad_(True) for k, v in P.items()}
+        s = RenderOptixSettings(None, False, None, None, None, None, None, cam, 1024, nsg, 0, 0, 0, ss, white, None)
+        img = RenderOptixFunction.apply(*(Q[k] for k in KEYS), s)
+        img.backward(dL)
+        torch.cuda.synchronize()
+        outs.append((img.detach().cpu(), {k: Q[k].grad.cpu() for k in KEYS if Q[k].grad is not None}))
+    assert outs[0][0].shape == (48 * 18, 3)
+    assert torch.equal(outs[0][0], outs[1][0])
+    for k, g in outs[0][1].items():
+        assert torch.equal(g, outs[1][1][k]), k
