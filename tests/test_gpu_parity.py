@@ -346,7 +346,8 @@ def test_fast_mode_bf16_storage_small_object_full_size(cuda, oracle):
 def test_supersampling_is_the_finer_ray_grid(cuda):
     """Supersampling (ssx, ssy) traces the image's W*ssx x H*ssy ray grid (optix_utils.py:132,
     168-169; forward/gaussians_aabb.cu:405-434): the same camera at twice the width gives the same rays, so
-    the (2, 1)-supersampled render and its gradients equal that camera's, bit for bit."""
+    the (2, 1)-supersampled image equals that camera's bit for bit, and so do the gradients up to the
+    summation order of the float atomics."""
     from ray_gauss_b200 import synthetic as S
     from ray_gauss_b200.optix_raycasting.render_optix import RenderOptixFunction, RenderOptixSettings
     p, _, white = S.workload("small_object", n=2000, seed=5)
@@ -366,5 +367,5 @@ def test_supersampling_is_the_finer_ray_grid(cuda):
         outs.append((img.detach().cpu(), {k: Q[k].grad.cpu() for k in KEYS if Q[k].grad is not None}))
     assert outs[0][0].shape == (48 * 18, 3)
     assert torch.equal(outs[0][0], outs[1][0])
-    for k, g in outs[0][1].items():
-        assert torch.equal(g, outs[1][1][k]), k
+    for k, g in outs[0][1].items():   # float atomics: equal up to their summation order
+        assert rel_l2(g.numpy(), outs[1][1][k].numpy()) <= 1e-5, k
