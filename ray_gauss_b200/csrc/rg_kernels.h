@@ -90,9 +90,7 @@ cudaError_t launch_color_backward(const rg_gaussians* g, const rg_camera* cams, 
 
 // mode: RG_MODE_PARITY / RG_MODE_FAST; cap: 64/128
 cudaError_t launch_render(bool backward, int mode, int cap, int grid, const RenderArgs& a, cudaStream_t s);
-int render_block_threads();
 int render_occupancy(bool backward, int mode, int cap);
-size_t render_smem_bytes(bool backward, int cap);
 
 // Copies a device status block read back to the host into the public struct (record_words is left
 // to the caller).

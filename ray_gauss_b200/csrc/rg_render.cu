@@ -1353,14 +1353,9 @@ cudaError_t launch_moment_grads(int n, const LeafRec* rec, const float4* ext, fl
     return cudaGetLastError();
 }
 
-int render_block_threads() { return kWarpsPerBlock * 32; }
-
 // List capacity per arithmetic: 4x the tuning value (64 or 128) for the fast lists; 128 for the
 // parity lists at either value (their per-lane slab ranges make an entry 64 B; shorter lists turn
 // dense slabs into multi-pass traversals, which the backward cannot replay).
-size_t render_smem_bytes(bool, int cap) {
-    return sizeof(WarpSmem<false, 128>) * kWarpsPerBlock;
-}
 static_assert(sizeof(WarpSmem<false, 128>) * kWarpsPerBlock <= 48 * 1024, "static shared memory limit");
 // the packet is read as float4: 16-byte aligned in every warp's slice of the block's array
 using ParitySmem = WarpSmem<false, 128>;
