@@ -396,3 +396,21 @@ def test_axis_aligned_views_against_oracle(cuda, oracle, mode):
                                               cv, W, H, white)
             assert np.abs(img - ref).max() <= tol, (axis, sign, float(np.abs(img - ref).max()))
             assert np.abs(ref - (1.0 if white else 0.0)).max() > 0.05   # the object is in view
+
+
+@pytest.mark.parametrize("n", [2, 3, 31, 32, 33, 100])
+def test_tiny_clouds_against_oracle(cuda, oracle, n):
+    """Clouds of a few Gaussians: a wide root with fewer than 32 children, leaves at uneven depths,
+    a second wide level from 33 on.  The parity images equal the oracle's."""
+    from ray_gauss_b200 import synthetic as S
+    p, _, white = S.workload("small_object", n=n, seed=n)
+    p["scales"] = p["scales"] * 6.0
+    P = {k: v.to(cuda).contiguous() for k, v in p.items()}
+    Pn = {k: v.cpu().numpy() for k, v in p.items()}
+    cam = S.sphere_camera(3.0, 32, 24, 40.0, seed=n, device=cuda)
+    img = _render(P, cam, white=white).detach().cpu().numpy()
+    cv = oracle.camera_vector(cam)
+    rgb = oracle.forward_sh(cv[:3], Pn["positions"], Pn["color_features"], None, None, None)
+    ref, _, _ = oracle.render_forward(Pn["positions"], Pn["scales"], Pn["quaternions"], Pn["densities"], rgb, cv,
+                                      32, 24, white)
+    assert np.abs(img - ref).max() <= IMG_TOL, float(np.abs(img - ref).max())
